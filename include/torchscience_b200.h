@@ -1,0 +1,146 @@
+/*
+ * torchscience_b200 — C ABI of the sm_100a special-function kernels.
+ *
+ * This library replaces the per-element CPU loops of torchscience's special
+ * functions (TensorIterator + at::native::cpu_kernel over the scalar templates
+ * in src/torchscience/csrc/kernel/special_functions/*.h, instantiated by
+ * src/torchscience/csrc/cpu/special_functions.h) with CUDA kernels.  It has no
+ * torch types in its signatures: every operand is a `tsb_tensor` (a device
+ * pointer plus sizes and element strides over the common iteration shape).
+ *
+ * Conventions shared by every entry point below:
+ *   - `in` / `out` hold n_in / n_out operands, in the order of the matching
+ *     torchscience schema (src/torchscience/csrc/torchscience.cpp), e.g. for
+ *     regularized_gamma_p_backward: in = {grad, a, x}, out = {grad_a, grad_x}.
+ *   - all operands share `ndim` and `sizes` (the broadcast iteration shape);
+ *     an input broadcast along a dim has stride 0 there.
+ *   - an OUTPUT with stride 0 along a dim of size > 1 is a reduced output: the
+ *     kernel sums the per-element values over that dim (deterministically, in
+ *     double, in a fixed order).  This is how backward kernels return
+ *     gradients already reduced to an input's shape.  Reduced outputs need a
+ *     device workspace of tsb_workspace_bytes(...) bytes.
+ *   - an output whose `data` is NULL is not requested and is not computed.
+ *   - all operands of one call have the same dtype.
+ *   - precision: TSB_PRECISION_AUTO picks the FP64 kernels for f64 data and
+ *     the mixed FP32 kernels (FP32 bulk, FP64 only in the classified bins that
+ *     need it) for f32/f16/bf16 data; TSB_PRECISION_FP64 runs the FP64
+ *     kernels for any dtype.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are
+ *     asynchronous and stream-ordered; the library keeps no per-call state.
+ *   - return value: TSB_OK or a negative tsb_status; tsb_last_error() gives a
+ *     message for the calling thread.  Nothing is launched on error.
+ */
+#ifndef TORCHSCIENCE_B200_H_
+#define TORCHSCIENCE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSB_MAX_DIMS 8
+
+typedef enum tsb_dtype {
+  TSB_F32 = 0,
+  TSB_F64 = 1,
+  TSB_F16 = 2,
+  TSB_BF16 = 3
+} tsb_dtype;
+
+typedef enum tsb_precision {
+  TSB_PRECISION_AUTO = 0,
+  TSB_PRECISION_FP64 = 1
+} tsb_precision;
+
+typedef enum tsb_status {
+  TSB_OK = 0,
+  TSB_ERR_ARGUMENT = -1,    /* null pointer, bad count, bad ndim/sizes */
+  TSB_ERR_DTYPE = -2,       /* unknown or mixed dtypes */
+  TSB_ERR_LAYOUT = -3,      /* reduced-output pattern this kernel cannot fuse */
+  TSB_ERR_WORKSPACE = -4,   /* workspace missing or too small */
+  TSB_ERR_LAUNCH = -5,      /* CUDA launch error */
+  TSB_ERR_DEVICE = -6       /* no usable sm_100 device */
+} tsb_status;
+
+typedef struct tsb_tensor {
+  void* data;                      /* device pointer to element [0,...,0] */
+  int32_t dtype;                   /* tsb_dtype */
+  int32_t ndim;                    /* 0 .. TSB_MAX_DIMS */
+  int64_t sizes[TSB_MAX_DIMS];     /* iteration shape */
+  int64_t strides[TSB_MAX_DIMS];   /* element strides (0 = broadcast/reduced) */
+} tsb_tensor;
+
+/* Library / error helpers. */
+const char* tsb_version(void);
+const char* tsb_last_error(void);
+const char* tsb_status_string(int32_t status);
+
+/* Bytes of device workspace (256-byte aligned) that an entry point called with
+ * these operands needs: 0 when no output is reduced, negative (a tsb_status)
+ * when the operands are invalid.  The reference has no counterpart: its CPU
+ * backward writes full-shape gradients and lets the autograd engine reduce
+ * them (cpu/macros.h:987-1032). */
+int64_t tsb_workspace_bytes(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_t n_out);
+
+/* Every op entry point has this signature. */
+#define TSB_OP_SIGNATURE(name)                                               \
+  int32_t name(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out,    \
+               int32_t n_out, int32_t precision, void* workspace,            \
+               int64_t workspace_bytes, void* stream)
+
+/* ---- Gamma family ------------------------------------------------------ */
+/* log_gamma(z): replaces kernel/special_functions/log_gamma.h:23-65, schema
+ * torchscience.cpp:849; backward log_gamma_backward.h:8-10 (:850),
+ * backward_backward log_gamma_backward_backward.h:11-20 (:851). */
+TSB_OP_SIGNATURE(tsb_log_gamma);
+TSB_OP_SIGNATURE(tsb_log_gamma_backward);
+TSB_OP_SIGNATURE(tsb_log_gamma_backward_backward);
+/* gamma(z): gamma.h:68-122, schema torchscience.cpp:813-815. */
+TSB_OP_SIGNATURE(tsb_gamma);
+TSB_OP_SIGNATURE(tsb_gamma_backward);
+TSB_OP_SIGNATURE(tsb_gamma_backward_backward);
+/* digamma(z): digamma.h:10-25, schema torchscience.cpp:817-819. */
+TSB_OP_SIGNATURE(tsb_digamma);
+TSB_OP_SIGNATURE(tsb_digamma_backward);
+TSB_OP_SIGNATURE(tsb_digamma_backward_backward);
+/* trigamma(z): trigamma.h:10-25 (+ tetragamma.h:11-30 in its backward),
+ * schema torchscience.cpp:821-823. */
+TSB_OP_SIGNATURE(tsb_trigamma);
+TSB_OP_SIGNATURE(tsb_trigamma_backward);
+TSB_OP_SIGNATURE(tsb_trigamma_backward_backward);
+
+/* ---- Regularized incomplete gamma ------------------------------------- */
+/* regularized_gamma_p(a, x): regularized_gamma_p.h:57-71, schema
+ * torchscience.cpp:853-855; backward regularized_gamma_p_backward.h:27-33,
+ * backward_backward regularized_gamma_p_backward_backward.h:12-41. */
+TSB_OP_SIGNATURE(tsb_regularized_gamma_p);
+TSB_OP_SIGNATURE(tsb_regularized_gamma_p_backward);
+TSB_OP_SIGNATURE(tsb_regularized_gamma_p_backward_backward);
+/* regularized_gamma_q(a, x): regularized_gamma_q.h:13-22, schema
+ * torchscience.cpp:857-859; backward regularized_gamma_q_backward.h:12-16,
+ * backward_backward regularized_gamma_q_backward_backward.h:12-22. */
+TSB_OP_SIGNATURE(tsb_regularized_gamma_q);
+TSB_OP_SIGNATURE(tsb_regularized_gamma_q_backward);
+TSB_OP_SIGNATURE(tsb_regularized_gamma_q_backward_backward);
+
+/* ---- Complete elliptic integrals --------------------------------------- */
+/* complete_legendre_elliptic_integral_k(m): complete_legendre_elliptic_integral_k.h:29-33,
+ * schema torchscience.cpp:1015-1017; backward ..._k_backward.h:24-53,
+ * backward_backward ..._k_backward_backward.h:13-126. */
+TSB_OP_SIGNATURE(tsb_complete_legendre_elliptic_integral_k);
+TSB_OP_SIGNATURE(tsb_complete_legendre_elliptic_integral_k_backward);
+TSB_OP_SIGNATURE(tsb_complete_legendre_elliptic_integral_k_backward_backward);
+/* complete_legendre_elliptic_integral_e(m): complete_legendre_elliptic_integral_e.h:28-36,
+ * schema torchscience.cpp:1019-1021; backward ..._e_backward.h:41-52,
+ * backward_backward ..._e_backward_backward.h:17-43. */
+TSB_OP_SIGNATURE(tsb_complete_legendre_elliptic_integral_e);
+TSB_OP_SIGNATURE(tsb_complete_legendre_elliptic_integral_e_backward);
+TSB_OP_SIGNATURE(tsb_complete_legendre_elliptic_integral_e_backward_backward);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* TORCHSCIENCE_B200_H_ */

@@ -1,0 +1,150 @@
+"""Generates the committed golden fixtures under tests/golden/.
+
+Run here, where the reference sources exist (the GPU box has only the
+fixtures):
+
+    python oracle/build_ref.py && python tests/golden/make_golden.py
+
+Each fixture holds seeded inputs drawn from the distributions of the
+benchmark configurations (SURVEY/BASELINE configs, small samples), the
+reference's own outputs for them (oracle/_ref/libref_scalar.so, i.e. the
+reference's scalar templates compiled from its sources) and high-accuracy
+values from scipy 1.18 / mpmath 1.3 ("truth").
+"""
+
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import mpmath as mp
+import numpy as np
+import scipy.special as sp
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from oracle import oracle as O  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+mp.mp.dps = 40
+
+
+def lu(rng, lo, hi, n):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+
+
+def ref(name, p, *ins):
+    r = O.reference(name, p, *ins)
+    if r is None:
+        raise SystemExit("oracle/_ref/libref_scalar.so missing: run python oracle/build_ref.py first")
+    return r
+
+
+def gamma_family():
+    rng = np.random.default_rng(0)
+    x = np.concatenate(
+        [
+            rng.uniform(0.01, 50.0, 2048),  # config 1 distribution
+            lu(rng, 0.1, 100.0, 1024),  # config 5 k distribution
+            rng.uniform(-20.0, 0.0, 256),  # reflection region
+            rng.uniform(1.3, 1.6, 128),  # around the digamma root
+            np.array([0.5, 1.0, 2.0, 3.0, 4.0, 5.0, 10.0, 100.0, 171.0, 1e-3, 1e-8]),
+        ]
+    )
+    g = rng.standard_normal(x.size)
+    d = {"x": x, "g": g}
+    for nm in ["log_gamma", "gamma", "digamma", "trigamma"]:
+        d[f"ref_{nm}"] = ref(nm, 0, x)[0]
+        d[f"ref_{nm}_backward"] = ref(nm, 1, g, x)[0]
+    d["truth_log_gamma"] = sp.gammaln(x)
+    d["truth_gamma"] = sp.gamma(x)
+    d["truth_digamma"] = sp.psi(x)
+    for k in (1, 2, 3):
+        d[f"truth_polygamma{k}"] = sp.polygamma(k, x)
+    # mpmath for the sign-carrying reflection region and the digamma root band
+    d["truth_digamma"] = np.array([float(mp.digamma(mp.mpf(v))) if v <= 0 or 1.3 < v < 1.6 else sp.psi(v) for v in x])
+    np.savez_compressed(OUT / "gamma_family.npz", **d)
+
+
+def igamma():
+    rng = np.random.default_rng(1)
+    a_grid = lu(rng, 1e-2, 1e3, 48)
+    x_grid = lu(rng, 1e-3, 2e3, 48)
+    A, X = np.meshgrid(a_grid, x_grid, indexing="ij")
+    a_s = lu(rng, 1e-2, 1e3, 1024)
+    x_s = a_s * (1.0 + rng.uniform(-1e-2, 1e-2, a_s.size))  # |x - a| < 1e-2 a stress set
+    a = np.concatenate([A.ravel(), a_s, [1.0, 1.0, 2.0, 0.5, 10.0]])
+    x = np.concatenate([X.ravel(), x_s, [0.0, 100.0, 1e-300, 0.25, 9.5]])
+    g = rng.standard_normal(a.size)
+    d = {"a": a, "x": x, "g": g}
+    for nm in ["regularized_gamma_p", "regularized_gamma_q"]:
+        d[f"ref_{nm}"] = ref(nm, 0, a, x)[0]
+        ga, gx = ref(nm, 1, g, a, x)
+        d[f"ref_{nm}_grad_a"], d[f"ref_{nm}_grad_x"] = ga, gx
+    d["truth_p"] = sp.gammainc(a, x)
+    d["truth_q"] = sp.gammaincc(a, x)
+    # Derivatives from mpmath at 40 digits on a subsample.
+    idx = rng.choice(a.size - 5, 160, replace=False)
+    d["deriv_idx"] = idx
+    pa, px, paa, pax, pxx = [], [], [], [], []
+    for i in idx:
+        ai, xi = mp.mpf(a[i]), mp.mpf(x[i])
+
+        def P(aa, xx):
+            return mp.gammainc(aa, 0, xx, regularized=True)
+
+        pa.append(float(mp.diff(lambda t: P(t, xi), ai)))
+        px.append(float(mp.exp((ai - 1) * mp.log(xi) - xi - mp.loggamma(ai))))
+        paa.append(float(mp.diff(lambda t: P(t, xi), ai, 2)))
+        pax.append(float(mp.diff(lambda t: mp.exp((t - 1) * mp.log(xi) - xi - mp.loggamma(t)), ai)))
+        pxx.append(float(px[-1] * ((ai - 1) / xi - 1)))
+    d["truth_pa"], d["truth_px"] = np.array(pa), np.array(px)
+    d["truth_paa"], d["truth_pax"], d["truth_pxx"] = np.array(paa), np.array(pax), np.array(pxx)
+    np.savez_compressed(OUT / "igamma.npz", **d)
+
+
+def elliptic():
+    rng = np.random.default_rng(2)
+    m = np.concatenate(
+        [
+            rng.uniform(0.0, 1.0 - 1e-9, 2048),  # config 5 distribution
+            1.0 - lu(rng, 1e-12, 1e-2, 256),  # near the logarithmic singularity
+            rng.uniform(-10.0, 0.0, 128),  # negative parameter
+            lu(rng, 1e-12, 0.1, 128),  # small m (series band)
+            np.array([0.0, 0.5, -1.0, 0.9]),
+        ]
+    )
+    g = rng.standard_normal(m.size)
+    d = {"m": m, "g": g}
+    for nm, key in [("complete_legendre_elliptic_integral_k", "k"), ("complete_legendre_elliptic_integral_e", "e")]:
+        d[f"ref_{key}"] = ref(nm, 0, m)[0]
+        d[f"ref_{key}_backward"] = ref(nm, 1, g, m)[0]
+    K = np.array([float(mp.ellipk(mp.mpf(v))) for v in m])
+    E = np.array([float(mp.ellipe(mp.mpf(v))) for v in m])
+    d["truth_k"], d["truth_e"] = K, E
+    dk, de, dkk, dee = [], [], [], []
+    for v in m:
+        mv = mp.mpf(v)
+        if mv == 0:
+            dk.append(float(mp.pi / 8))
+            de.append(float(-mp.pi / 8))
+            dkk.append(float(9 * mp.pi / 64))
+            dee.append(float(-3 * mp.pi / 64))
+            continue
+        k, e = mp.ellipk(mv), mp.ellipe(mv)
+        kp = (e - (1 - mv) * k) / (2 * mv * (1 - mv))
+        ep = (e - k) / (2 * mv)
+        dk.append(float(kp))
+        de.append(float(ep))
+        dkk.append(float(mp.diff(mp.ellipk, mv, 2)))
+        dee.append(float(mp.diff(mp.ellipe, mv, 2)))
+    d["truth_dk"], d["truth_de"] = np.array(dk), np.array(de)
+    d["truth_dkk"], d["truth_dee"] = np.array(dkk), np.array(dee)
+    np.savez_compressed(OUT / "elliptic.npz", **d)
+
+
+if __name__ == "__main__":
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic"]
+    for w in which:
+        globals()[w]()
+        print("wrote", w)

@@ -1,0 +1,87 @@
+"""The oracle pinned before it is trusted: the C restatement against the
+reference's own outputs (golden fixtures made from the reference's compiled
+scalar kernels) and against the known-answer tests in the reference's test
+suite; the reference's accuracy bands against scipy/mpmath."""
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._util import golden, rel_err, ulp_err
+
+
+@pytest.mark.parametrize("name", ["log_gamma", "gamma", "digamma", "trigamma"])
+def test_restatement_matches_reference_outputs_gamma_family(name):
+    d = golden("gamma_family")
+    x = d["x"]
+    m = x > 0  # the reference's real recurrences are the restated ones for x > 0
+    got = O.restated(name, 0, x[m])[0]
+    assert ulp_err(got, d[f"ref_{name}"][m]).max() <= 2
+    if name != "gamma":
+        got = O.restated(name, 1, d["g"][m], x[m])[0]
+        assert ulp_err(got, d[f"ref_{name}_backward"][m]).max() <= 2
+
+
+@pytest.mark.parametrize("name,key", [("regularized_gamma_p", "p"), ("regularized_gamma_q", "q")])
+def test_restatement_matches_reference_outputs_igamma(name, key):
+    d = golden("igamma")
+    got = O.restated(name, 0, d["a"], d["x"])[0]
+    assert ulp_err(got, d[f"ref_{name}"]).max() <= 2
+    ga, gx = O.restated(name, 1, d["g"], d["a"], d["x"])
+    assert ulp_err(ga, d[f"ref_{name}_grad_a"]).max() <= 2
+    assert ulp_err(gx, d[f"ref_{name}_grad_x"]).max() <= 2
+
+
+@pytest.mark.parametrize("name,key", [("complete_legendre_elliptic_integral_k", "k"), ("complete_legendre_elliptic_integral_e", "e")])
+def test_restatement_matches_reference_outputs_elliptic(name, key):
+    d = golden("elliptic")
+    got = O.restated(name, 0, d["m"])[0]
+    assert ulp_err(got, d[f"ref_{key}"]).max() <= 2
+
+
+def test_known_answers_from_reference_tests():
+    # test__log_gamma.py:149-165 known values and half value
+    z = np.array([1.0, 2.0, 3.0, 4.0, 5.0, 0.5])
+    want = np.array([0.0, 0.0, math.log(2), math.log(6), math.log(24), 0.5 * math.log(math.pi)])
+    np.testing.assert_allclose(O.restated("log_gamma", 0, z)[0], want, rtol=1e-8, atol=1e-8)
+    # test__log_gamma.py:178-183 recurrence lnΓ(z+1) = lnΓ(z) + ln z
+    z = np.array([0.5, 1.5, 2.5, 5.0, 10.0])
+    np.testing.assert_allclose(O.restated("log_gamma", 0, z + 1)[0], O.restated("log_gamma", 0, z)[0] + np.log(z), rtol=1e-10, atol=1e-10)
+    # test__log_gamma.py:185-192 pole at 0
+    assert np.isinf(O.restated("log_gamma", 0, np.array([0.0]))[0]).all()
+    # test__regularized_gamma_p.py:30-56: P(a,0)=0, P(1,x)=1-e^-x, P(a,100)->1, range
+    a = np.array([0.5, 1.0, 2.0, 10.0])
+    assert np.all(O.restated("regularized_gamma_p", 0, a, 0 * a)[0] == 0)
+    x = np.linspace(0.1, 5.0, 50)
+    np.testing.assert_allclose(O.restated("regularized_gamma_p", 0, np.ones_like(x), x)[0], 1 - np.exp(-x), atol=1e-6)
+    np.testing.assert_allclose(O.restated("regularized_gamma_p", 0, np.array([1.0, 2.0, 5.0]), np.full(3, 100.0))[0], 1.0, atol=1e-10)
+    rng = np.random.default_rng(0)
+    p = O.restated("regularized_gamma_p", 0, rng.random(100) * 10 + 0.1, rng.random(100) * 20)[0]
+    assert np.all((p >= 0) & (p <= 1))
+
+
+def test_reference_accuracy_bands():
+    """Where the reference is accurate (parity at 4 ulp + its own error is meaningful)
+    and where it is not (graded against scipy/mpmath only)."""
+    g = golden("gamma_family")
+    x = g["x"]
+    pos = x > 0
+    zero_band = (np.abs(x - 1) < 0.1) | (np.abs(x - 2) < 0.1)
+    e = rel_err(g["ref_log_gamma"], g["truth_log_gamma"])
+    assert e[pos & ~zero_band].max() < 1e-13
+    e = rel_err(g["ref_gamma"], g["truth_gamma"])
+    assert e[pos & (x < 100)].max() < 1e-12
+    # digamma: truncated 3-term asymptotic -> ~1e-8 (defect band)
+    e = rel_err(g["ref_digamma"], g["truth_digamma"])
+    assert 1e-10 < np.median(e[pos & (x < 5)])
+    ig = golden("igamma")
+    e = rel_err(ig["ref_regularized_gamma_p"], ig["truth_p"], floor=1e-280)
+    assert np.nanmax(e[ig["truth_p"] > 1e-280]) < 1e-8
+    el = golden("elliptic")
+    m = el["m"]
+    inside = (m >= 0) & (m < 1 - 1e-12)
+    assert rel_err(el["ref_k"], el["truth_k"])[inside].max() < 1e-13
+    # E(1) and m -> 1 are where the reference's R_G form loses accuracy
+    assert rel_err(el["ref_e"], el["truth_e"])[inside].max() < 1e-12

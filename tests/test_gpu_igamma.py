@@ -1,0 +1,143 @@
+"""Regularized incomplete gamma P/Q through the C ABI on the GPU: values against
+scipy, parity with the reference, analytic derivatives against mpmath, mixed
+against FP64, fused broadcast-reduced gradients, gradcheck/gradgradcheck."""
+
+import numpy as np
+import pytest
+import torch
+
+import torchscience_b200  # noqa: F401
+from tests._util import golden, rel_err, run
+
+pytestmark = pytest.mark.gpu
+
+D = golden("igamma")
+A, X, G = D["a"], D["x"], D["g"]
+
+
+def cuda(a, dtype=torch.float64):
+    return torch.tensor(np.asarray(a), dtype=dtype, device="cuda")
+
+
+def test_fp64_values_against_scipy():
+    (p,) = run("regularized_gamma_p", cuda(A), cuda(X))
+    (q,) = run("regularized_gamma_q", cuda(A), cuda(X))
+    p, q = p.cpu().numpy(), q.cpu().numpy()
+    tp, tq = D["truth_p"], D["truth_q"]
+    mp_ = tp > 1e-290
+    mq = tq > 1e-290
+    ep = rel_err(p, tp)[mp_]
+    eq = rel_err(q, tq)[mq]
+    assert ep.max() <= 1e-12, f"P max rel err {ep.max():.3e}"
+    # Q = 1 - P in the series region loses digits only when P -> 1 (small a); cap at 1e-10
+    assert eq.max() <= 1e-10, f"Q max rel err {eq.max():.3e}"
+    assert np.all(np.abs(p + q - 1) <= 4e-16)
+
+
+def test_fp64_parity_with_reference():
+    """|ours - ref| <= 4 ulp + |ref - truth| (the reference is accurate to ~1e-10 here)."""
+    (p,) = run("regularized_gamma_p", cuda(A), cuda(X))
+    p = p.cpu().numpy()
+    ref, tru = D["ref_regularized_gamma_p"], D["truth_p"]
+    allowed = 4 * np.spacing(np.abs(ref)) + np.abs(ref - tru) + 4 * np.spacing(np.abs(tru))
+    assert np.all(np.abs(p - ref) <= allowed)
+
+
+def test_fp64_derivatives_against_mpmath():
+    i = D["deriv_idx"]
+    a, x = cuda(A[i]), cuda(X[i])
+    one = torch.ones_like(a)
+    ga, gx = run("regularized_gamma_p_backward", one, a, x, n_out=2)
+    m = np.abs(D["truth_pa"]) > 1e-290
+    e = rel_err(ga.cpu().numpy(), D["truth_pa"])[m]
+    assert e.max() <= 1e-10, f"dP/da {e.max():.3e}"
+    assert rel_err(gx.cpu().numpy(), D["truth_px"]).max() <= 1e-12
+    # second derivatives through the double-backward entry point
+    z = torch.zeros_like(a)
+    o_g, o_a, o_x = run("regularized_gamma_p_backward_backward", one, z, one, a, x, n_out=3)  # gga=1, ggx=0
+    m2 = np.abs(D["truth_paa"]) > 1e-280
+    e2 = rel_err(o_a.cpu().numpy(), D["truth_paa"])[m2]
+    assert np.median(e2) <= 1e-10 and e2.max() <= 1e-6, f"d2P/da2 {e2.max():.3e}"
+    assert rel_err(o_x.cpu().numpy(), D["truth_pax"])[np.abs(D["truth_pax"]) > 1e-280].max() <= 1e-10
+    _, _, o_xx = run("regularized_gamma_p_backward_backward", z, one, one, a, x, n_out=3)  # ggx=1
+    assert rel_err(o_xx.cpu().numpy(), D["truth_pxx"])[np.abs(D["truth_pxx"]) > 1e-280].max() <= 1e-11
+
+
+def test_q_derivatives_are_negated_p_derivatives():
+    a, x, g = cuda(A), cuda(X), cuda(G)
+    pa, px = run("regularized_gamma_p_backward", g, a, x, n_out=2)
+    qa, qx = run("regularized_gamma_q_backward", g, a, x, n_out=2)
+    assert torch.equal(pa, -qa) and torch.equal(px, -qx)
+
+
+def test_mixed_within_1e6_of_fp64():
+    a32, x32 = A.astype(np.float32), X.astype(np.float32)
+    (pm,) = run("regularized_gamma_p", cuda(a32, torch.float32), cuda(x32, torch.float32))
+    (pd,) = run("regularized_gamma_p", cuda(a32.astype(np.float64)), cuda(x32.astype(np.float64)))
+    pm, pd = pm.cpu().numpy().astype(np.float64), pd.cpu().numpy()
+    m = pd > 1e-30  # below float32's normal range the relative error is not meaningful
+    e = rel_err(pm, pd)[m]
+    assert e.max() <= 1e-6, f"mixed P {e.max():.3e}"
+    g32 = G.astype(np.float32)
+    gm = run("regularized_gamma_p_backward", cuda(g32, torch.float32), cuda(a32, torch.float32), cuda(x32, torch.float32), n_out=2)
+    gd = run("regularized_gamma_p_backward", cuda(g32.astype(np.float64)), cuda(a32.astype(np.float64)), cuda(x32.astype(np.float64)), n_out=2)
+    for k in range(2):
+        u, v = gm[k].cpu().numpy().astype(np.float64), gd[k].cpu().numpy()
+        mm = np.abs(v) > 1e-30
+        e = rel_err(u, v)[mm]
+        assert e.max() <= 1e-6, f"mixed grad {k}: {e.max():.3e}"
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_fused_reduced_gradients_match_full_gradients(dtype):
+    """Config-2 broadcast layout (R,1) x (1,C): gradients reduced in-kernel
+    (deterministic two-stage sum) equal the full-shape gradients summed."""
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    R, C = 1000, 777
+    a = torch.exp(torch.empty(R, 1, device="cuda", dtype=torch.float64).uniform_(np.log(1e-2), np.log(1e3), generator=gen)).to(dtype)
+    x = torch.exp(torch.empty(1, C, device="cuda", dtype=torch.float64).uniform_(np.log(1e-3), np.log(2e3), generator=gen)).to(dtype)
+    g = torch.randn(R, C, device="cuda", dtype=dtype, generator=gen)
+    ga, gx = run("regularized_gamma_p_backward", g, a, x, n_out=2, out_shapes=[a.shape, x.shape])
+    fa, fx = run("regularized_gamma_p_backward", g, a, x, n_out=2)
+    ra = fa.double().sum(1, keepdim=True)
+    rx = fx.double().sum(0, keepdim=True)
+    tol = 1e-12 if dtype == torch.float64 else 1e-5
+    assert torch.allclose(ga.double(), ra, rtol=tol, atol=tol * ra.abs().max().item())
+    assert torch.allclose(gx.double(), rx, rtol=tol, atol=tol * rx.abs().max().item())
+    # deterministic: bitwise identical on a second call
+    ga2, gx2 = run("regularized_gamma_p_backward", g, a, x, n_out=2, out_shapes=[a.shape, x.shape])
+    assert torch.equal(ga, ga2) and torch.equal(gx, gx2)
+
+
+def test_autograd_reduced_path_and_gradcheck():
+    from torchscience_b200 import special_functions as sf
+
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    a = (torch.rand(6, 1, device="cuda", dtype=torch.float64, generator=gen) * 5 + 0.2).requires_grad_()
+    x = (torch.rand(1, 5, device="cuda", dtype=torch.float64, generator=gen) * 8 + 0.05).requires_grad_()
+    y = sf.regularized_gamma_p(a, x)
+    ga, gx = torch.autograd.grad(y.sum(), (a, x))
+    fa, fx = run("regularized_gamma_p_backward", torch.ones(6, 5, device="cuda", dtype=torch.float64), a.detach(), x.detach(), n_out=2)
+    assert torch.allclose(ga, fa.sum(1, keepdim=True), rtol=1e-13)
+    assert torch.allclose(gx, fx.sum(0, keepdim=True), rtol=1e-13)
+    assert torch.autograd.gradcheck(sf.regularized_gamma_p, (a, x), eps=1e-6, atol=1e-7, rtol=1e-5)
+    assert torch.autograd.gradgradcheck(sf.regularized_gamma_p, (a, x), eps=1e-6, atol=1e-6, rtol=1e-4)
+    assert torch.autograd.gradcheck(sf.regularized_gamma_q, (a, x), eps=1e-6, atol=1e-7, rtol=1e-5)
+
+
+def test_full_size_properties_config2():
+    """At the benchmark size (4096 x 4096 broadcast + 2^20 stress points):
+    P + Q = 1, 0 <= P <= 1, and the recurrence P(a+1,x) = P(a,x) - x^a e^-x / Γ(a+1)."""
+    from torchscience_b200 import special_functions as sf
+
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    a = torch.exp(torch.empty(4096, 1, device="cuda", dtype=torch.float64).uniform_(np.log(1e-2), np.log(1e3), generator=gen))
+    x = torch.exp(torch.empty(1, 4096, device="cuda", dtype=torch.float64).uniform_(np.log(1e-3), np.log(2e3), generator=gen))
+    p = sf.regularized_gamma_p(a, x)
+    q = sf.regularized_gamma_q(a, x)
+    assert ((p + q - 1).abs().max().item()) <= 4e-16
+    assert p.min().item() >= 0 and p.max().item() <= 1
+    p1 = sf.regularized_gamma_p(a + 1, x)
+    d = torch.exp(a * torch.log(x) - x - torch.lgamma(a + 1))
+    r = (p1 - (p - d)).abs()
+    assert r.max().item() <= 1e-12

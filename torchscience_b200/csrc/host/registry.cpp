@@ -1,0 +1,287 @@
+// torch.ops.torchscience.* registration for the B200 kernels.
+//
+// The schema strings are the reference's own (src/torchscience/csrc/torchscience.cpp,
+// cited per op below) so that torch.ops.torchscience.<op>, <op>_backward and
+// <op>_backward_backward keep their names, argument names and return arity.
+// Implementations are registered for CUDA (the sm_100a kernels through the C
+// ABI), Meta (shape/dtype via TensorIterator, as meta/macros.h:9-411 does),
+// Autograd (the same Function pair structure as autograd/macros.h:5-837),
+// AutocastCUDA (cast to float32 like autocast/macros.h:6-172) and CPU (an
+// error: there is no CPU fallback).
+#include <ATen/autocast_mode.h>
+#include <torch/autograd.h>
+#include <torch/library.h>
+
+#include "pointwise.h"
+#include "schemas.h"
+
+using torch::autograd::AutogradContext;
+using torch::autograd::variable_list;
+
+namespace tsbh {
+
+inline bool wants_grad(const at::Tensor& t) {
+  return t.requires_grad() && (at::isFloatingType(t.scalar_type()) || at::isComplexType(t.scalar_type()));
+}
+
+inline bool any_cuda(std::initializer_list<at::Tensor> ts) {
+  for (const auto& t : ts)
+    if (t.defined() && t.is_cuda()) return true;
+  return false;
+}
+
+}  // namespace tsbh
+
+// ---------------------------------------------------------------- unary ops
+// Name: op name; Cls: autograd class prefix; A: argument name in the schema.
+#define TSBH_UNARY_OP(name, Cls, A, FWD, BWD, BB)                                                       \
+  namespace tsbh::ops {                                                                                 \
+  at::Tensor name##_cuda(const at::Tensor& a) { return run_pointwise(FWD, #name, {a}, 1)[0]; }         \
+  at::Tensor name##_backward_cuda(const at::Tensor& g, const at::Tensor& a) {                          \
+    return run_pointwise(BWD, #name "_backward", {g, a}, 1)[0];                                        \
+  }                                                                                                     \
+  std::tuple<at::Tensor, at::Tensor> name##_backward_backward_cuda(const at::Tensor& gg, const at::Tensor& g, \
+                                                                    const at::Tensor& a) {            \
+    if (!gg.defined()) return {};                                                                      \
+    auto r = run_pointwise(BB, #name "_backward_backward", {gg, g, a}, 2);                             \
+    return {r[0], r[1]};                                                                               \
+  }                                                                                                     \
+  at::Tensor name##_meta(const at::Tensor& a) { return meta_pointwise(#name, {a}, 1)[0]; }             \
+  at::Tensor name##_backward_meta(const at::Tensor& g, const at::Tensor& a) {                          \
+    return meta_pointwise(#name "_backward", {g, a}, 1)[0];                                            \
+  }                                                                                                     \
+  std::tuple<at::Tensor, at::Tensor> name##_backward_backward_meta(const at::Tensor& gg, const at::Tensor& g, \
+                                                                    const at::Tensor& a) {            \
+    if (!gg.defined()) return {};                                                                      \
+    auto r = meta_pointwise(#name "_backward_backward", {gg, g, a}, 2);                                \
+    return {r[0], r[1]};                                                                               \
+  }                                                                                                     \
+  at::Tensor name##_cpu(const at::Tensor&) { cpu_not_supported(#name); }                               \
+  at::Tensor name##_backward_cpu(const at::Tensor&, const at::Tensor&) { cpu_not_supported(#name "_backward"); } \
+  std::tuple<at::Tensor, at::Tensor> name##_backward_backward_cpu(const at::Tensor&, const at::Tensor&,      \
+                                                                   const at::Tensor&) {               \
+    cpu_not_supported(#name "_backward_backward");                                                     \
+  }                                                                                                     \
+  class Cls##Backward : public torch::autograd::Function<Cls##Backward> {                              \
+   public:                                                                                              \
+    static variable_list forward(AutogradContext* ctx, const at::Tensor& g, const at::Tensor& a, bool req) { \
+      ctx->save_for_backward({g, a});                                                                  \
+      ctx->saved_data["req"] = req;                                                                    \
+      at::AutoDispatchBelowAutograd guard;                                                             \
+      static auto op = c10::Dispatcher::singleton()                                                    \
+                           .findSchemaOrThrow("torchscience::" #name "_backward", "")                  \
+                           .typed<at::Tensor(const at::Tensor&, const at::Tensor&)>();                 \
+      return {op.call(g, a)};                                                                          \
+    }                                                                                                   \
+    static variable_list backward(AutogradContext* ctx, const variable_list& go) {                     \
+      auto saved = ctx->get_saved_variables();                                                          \
+      const bool req = ctx->saved_data["req"].toBool();                                                \
+      if (!go[0].defined() || !req) return {at::Tensor(), at::Tensor(), at::Tensor()};                 \
+      at::AutoDispatchBelowAutograd guard;                                                             \
+      static auto op = c10::Dispatcher::singleton()                                                    \
+                           .findSchemaOrThrow("torchscience::" #name "_backward_backward", "")         \
+                           .typed<std::tuple<at::Tensor, at::Tensor>(const at::Tensor&, const at::Tensor&, \
+                                                                     const at::Tensor&)>();           \
+      auto [gg_out, g_a] = op.call(go[0], saved[0], saved[1]);                                         \
+      return {gg_out, g_a, at::Tensor()};                                                              \
+    }                                                                                                   \
+  };                                                                                                    \
+  class Cls : public torch::autograd::Function<Cls> {                                                  \
+   public:                                                                                              \
+    static at::Tensor forward(AutogradContext* ctx, const at::Tensor& a) {                             \
+      ctx->save_for_backward({a});                                                                     \
+      ctx->saved_data["req"] = wants_grad(a);                                                          \
+      at::AutoDispatchBelowAutograd guard;                                                             \
+      static auto op = c10::Dispatcher::singleton()                                                    \
+                           .findSchemaOrThrow("torchscience::" #name, "")                              \
+                           .typed<at::Tensor(const at::Tensor&)>();                                    \
+      return op.call(a);                                                                               \
+    }                                                                                                   \
+    static variable_list backward(AutogradContext* ctx, const variable_list& go) {                     \
+      auto saved = ctx->get_saved_variables();                                                          \
+      const bool req = ctx->saved_data["req"].toBool();                                                \
+      auto g = Cls##Backward::apply(go[0], saved[0], req);                                             \
+      return {req ? g[0] : at::Tensor()};                                                              \
+    }                                                                                                   \
+  };                                                                                                    \
+  at::Tensor name##_autograd(const at::Tensor& a) { return Cls::apply(a); }                            \
+  at::Tensor name##_autocast(const at::Tensor& a) {                                                    \
+    c10::impl::ExcludeDispatchKeyGuard no_autocast(c10::DispatchKey::AutocastCUDA);                    \
+    static auto op = c10::Dispatcher::singleton()                                                      \
+                         .findSchemaOrThrow("torchscience::" #name, "")                                \
+                         .typed<at::Tensor(const at::Tensor&)>();                                      \
+    return op.call(at::autocast::cached_cast(at::kFloat, a, c10::DeviceType::CUDA));                   \
+  }                                                                                                     \
+  } /* namespace tsbh::ops */                                                                           \
+  TORCH_LIBRARY_IMPL(torchscience, CUDA, m) {                                                           \
+    m.impl(#name, tsbh::ops::name##_cuda);                                                              \
+    m.impl(#name "_backward", tsbh::ops::name##_backward_cuda);                                         \
+    m.impl(#name "_backward_backward", tsbh::ops::name##_backward_backward_cuda);                       \
+  }                                                                                                     \
+  TORCH_LIBRARY_IMPL(torchscience, Meta, m) {                                                           \
+    m.impl(#name, tsbh::ops::name##_meta);                                                              \
+    m.impl(#name "_backward", tsbh::ops::name##_backward_meta);                                         \
+    m.impl(#name "_backward_backward", tsbh::ops::name##_backward_backward_meta);                       \
+  }                                                                                                     \
+  TORCH_LIBRARY_IMPL(torchscience, CPU, m) {                                                            \
+    m.impl(#name, tsbh::ops::name##_cpu);                                                               \
+    m.impl(#name "_backward", tsbh::ops::name##_backward_cpu);                                          \
+    m.impl(#name "_backward_backward", tsbh::ops::name##_backward_backward_cpu);                        \
+  }                                                                                                     \
+  TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl(#name, tsbh::ops::name##_autograd); }         \
+  TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl(#name, tsbh::ops::name##_autocast); }
+
+// --------------------------------------------------------------- binary ops
+#define TSBH_BINARY_OP(name, Cls, A, B, FWD, BWD, BB)                                                   \
+  namespace tsbh::ops {                                                                                 \
+  at::Tensor name##_cuda(const at::Tensor& a, const at::Tensor& b) {                                   \
+    return run_pointwise(FWD, #name, {a, b}, 1)[0];                                                    \
+  }                                                                                                     \
+  std::tuple<at::Tensor, at::Tensor> name##_backward_cuda(const at::Tensor& g, const at::Tensor& a,    \
+                                                           const at::Tensor& b) {                      \
+    auto r = run_pointwise(BWD, #name "_backward", {g, a, b}, 2);                                      \
+    return {r[0], r[1]};                                                                               \
+  }                                                                                                     \
+  std::tuple<at::Tensor, at::Tensor, at::Tensor> name##_backward_backward_cuda(                        \
+      const at::Tensor& gga, const at::Tensor& ggb, const at::Tensor& g, const at::Tensor& a, const at::Tensor& b) { \
+    auto r = run_pointwise(BB, #name "_backward_backward", {gga, ggb, g, a, b}, 3);                   \
+    return {r[0], r[1], r[2]};                                                                         \
+  }                                                                                                     \
+  at::Tensor name##_meta(const at::Tensor& a, const at::Tensor& b) {                                   \
+    return meta_pointwise(#name, {a, b}, 1)[0];                                                        \
+  }                                                                                                     \
+  std::tuple<at::Tensor, at::Tensor> name##_backward_meta(const at::Tensor& g, const at::Tensor& a,    \
+                                                           const at::Tensor& b) {                      \
+    auto r = meta_pointwise(#name "_backward", {g, a, b}, 2);                                          \
+    return {r[0], r[1]};                                                                               \
+  }                                                                                                     \
+  std::tuple<at::Tensor, at::Tensor, at::Tensor> name##_backward_backward_meta(                        \
+      const at::Tensor& gga, const at::Tensor& ggb, const at::Tensor& g, const at::Tensor& a, const at::Tensor& b) { \
+    auto r = meta_pointwise(#name "_backward_backward", {gga, ggb, g, a, b}, 3);                      \
+    return {r[0], r[1], r[2]};                                                                         \
+  }                                                                                                     \
+  at::Tensor name##_cpu(const at::Tensor&, const at::Tensor&) { cpu_not_supported(#name); }            \
+  std::tuple<at::Tensor, at::Tensor> name##_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&) { \
+    cpu_not_supported(#name "_backward");                                                              \
+  }                                                                                                     \
+  std::tuple<at::Tensor, at::Tensor, at::Tensor> name##_backward_backward_cpu(                         \
+      const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&) { \
+    cpu_not_supported(#name "_backward_backward");                                                     \
+  }                                                                                                     \
+  class Cls##Backward : public torch::autograd::Function<Cls##Backward> {                              \
+   public:                                                                                              \
+    static variable_list forward(AutogradContext* ctx, const at::Tensor& g, const at::Tensor& a,       \
+                                 const at::Tensor& b, bool ra, bool rb) {                              \
+      ctx->save_for_backward({g, a, b});                                                               \
+      ctx->saved_data["ra"] = ra;                                                                      \
+      ctx->saved_data["rb"] = rb;                                                                      \
+      at::AutoDispatchBelowAutograd guard;                                                             \
+      if (any_cuda({g, a, b})) {                                                                       \
+        /* Gradients come back already reduced to a's and b's shapes. */                               \
+        return run_reduced_backward(BWD, #name "_backward", g, {a, b}, {ra, rb});                      \
+      }                                                                                                 \
+      static auto op = c10::Dispatcher::singleton()                                                    \
+                           .findSchemaOrThrow("torchscience::" #name "_backward", "")                  \
+                           .typed<std::tuple<at::Tensor, at::Tensor>(const at::Tensor&, const at::Tensor&, \
+                                                                     const at::Tensor&)>();           \
+      auto [ga, gb] = op.call(g, a, b);                                                                \
+      return {ga, gb};                                                                                 \
+    }                                                                                                   \
+    static variable_list backward(AutogradContext* ctx, const variable_list& go) {                     \
+      auto saved = ctx->get_saved_variables();                                                          \
+      const bool ra = ctx->saved_data["ra"].toBool(), rb = ctx->saved_data["rb"].toBool();             \
+      if ((!go[0].defined() && !go[1].defined()) || (!ra && !rb))                                      \
+        return {at::Tensor(), at::Tensor(), at::Tensor(), at::Tensor(), at::Tensor()};                 \
+      at::AutoDispatchBelowAutograd guard;                                                             \
+      auto gga = go[0].defined() ? go[0] : at::zeros_like(saved[1]);                                   \
+      auto ggb = go[1].defined() ? go[1] : at::zeros_like(saved[2]);                                   \
+      static auto op = c10::Dispatcher::singleton()                                                    \
+                           .findSchemaOrThrow("torchscience::" #name "_backward_backward", "")         \
+                           .typed<std::tuple<at::Tensor, at::Tensor, at::Tensor>(                      \
+                               const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&, \
+                               const at::Tensor&)>();                                                  \
+      auto [gg_out, g_a, g_b] = op.call(gga, ggb, saved[0], saved[1], saved[2]);                       \
+      return {gg_out, g_a, g_b, at::Tensor(), at::Tensor()};                                           \
+    }                                                                                                   \
+  };                                                                                                    \
+  class Cls : public torch::autograd::Function<Cls> {                                                  \
+   public:                                                                                              \
+    static at::Tensor forward(AutogradContext* ctx, const at::Tensor& a, const at::Tensor& b) {        \
+      ctx->save_for_backward({a, b});                                                                  \
+      ctx->saved_data["ra"] = wants_grad(a);                                                           \
+      ctx->saved_data["rb"] = wants_grad(b);                                                           \
+      at::AutoDispatchBelowAutograd guard;                                                             \
+      static auto op = c10::Dispatcher::singleton()                                                    \
+                           .findSchemaOrThrow("torchscience::" #name, "")                              \
+                           .typed<at::Tensor(const at::Tensor&, const at::Tensor&)>();                 \
+      return op.call(a, b);                                                                            \
+    }                                                                                                   \
+    static variable_list backward(AutogradContext* ctx, const variable_list& go) {                     \
+      auto saved = ctx->get_saved_variables();                                                          \
+      const bool ra = ctx->saved_data["ra"].toBool(), rb = ctx->saved_data["rb"].toBool();             \
+      auto g = Cls##Backward::apply(go[0], saved[0], saved[1], ra, rb);                                \
+      return {ra ? g[0] : at::Tensor(), rb ? g[1] : at::Tensor()};                                     \
+    }                                                                                                   \
+  };                                                                                                    \
+  at::Tensor name##_autograd(const at::Tensor& a, const at::Tensor& b) { return Cls::apply(a, b); }     \
+  at::Tensor name##_autocast(const at::Tensor& a, const at::Tensor& b) {                               \
+    c10::impl::ExcludeDispatchKeyGuard no_autocast(c10::DispatchKey::AutocastCUDA);                    \
+    const auto t = at::autocast::promote_type(at::kFloat, c10::DeviceType::CUDA, a, b);                \
+    static auto op = c10::Dispatcher::singleton()                                                      \
+                         .findSchemaOrThrow("torchscience::" #name, "")                                \
+                         .typed<at::Tensor(const at::Tensor&, const at::Tensor&)>();                   \
+    return op.call(at::autocast::cached_cast(t, a, c10::DeviceType::CUDA),                             \
+                   at::autocast::cached_cast(t, b, c10::DeviceType::CUDA));                            \
+  }                                                                                                     \
+  } /* namespace tsbh::ops */                                                                           \
+  TORCH_LIBRARY_IMPL(torchscience, CUDA, m) {                                                           \
+    m.impl(#name, tsbh::ops::name##_cuda);                                                              \
+    m.impl(#name "_backward", tsbh::ops::name##_backward_cuda);                                         \
+    m.impl(#name "_backward_backward", tsbh::ops::name##_backward_backward_cuda);                       \
+  }                                                                                                     \
+  TORCH_LIBRARY_IMPL(torchscience, Meta, m) {                                                           \
+    m.impl(#name, tsbh::ops::name##_meta);                                                              \
+    m.impl(#name "_backward", tsbh::ops::name##_backward_meta);                                         \
+    m.impl(#name "_backward_backward", tsbh::ops::name##_backward_backward_meta);                       \
+  }                                                                                                     \
+  TORCH_LIBRARY_IMPL(torchscience, CPU, m) {                                                            \
+    m.impl(#name, tsbh::ops::name##_cpu);                                                               \
+    m.impl(#name "_backward", tsbh::ops::name##_backward_cpu);                                          \
+    m.impl(#name "_backward_backward", tsbh::ops::name##_backward_backward_cpu);                        \
+  }                                                                                                     \
+  TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl(#name, tsbh::ops::name##_autograd); }         \
+  TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl(#name, tsbh::ops::name##_autocast); }
+
+// Schemas: identical strings to the reference's TORCH_LIBRARY block.
+TORCH_LIBRARY(torchscience, m) { TSB_DEFINE_TORCHSCIENCE_SCHEMAS(m) }
+
+TSBH_UNARY_OP(log_gamma, LogGamma, z, tsb_log_gamma, tsb_log_gamma_backward, tsb_log_gamma_backward_backward)
+TSBH_UNARY_OP(gamma, Gamma, z, tsb_gamma, tsb_gamma_backward, tsb_gamma_backward_backward)
+TSBH_UNARY_OP(digamma, Digamma, z, tsb_digamma, tsb_digamma_backward, tsb_digamma_backward_backward)
+TSBH_UNARY_OP(trigamma, Trigamma, z, tsb_trigamma, tsb_trigamma_backward, tsb_trigamma_backward_backward)
+TSBH_BINARY_OP(regularized_gamma_p, RegularizedGammaP, a, x, tsb_regularized_gamma_p, tsb_regularized_gamma_p_backward,
+               tsb_regularized_gamma_p_backward_backward)
+TSBH_BINARY_OP(regularized_gamma_q, RegularizedGammaQ, a, x, tsb_regularized_gamma_q, tsb_regularized_gamma_q_backward,
+               tsb_regularized_gamma_q_backward_backward)
+TSBH_UNARY_OP(complete_legendre_elliptic_integral_k, CompleteLegendreEllipticIntegralK, m,
+              tsb_complete_legendre_elliptic_integral_k, tsb_complete_legendre_elliptic_integral_k_backward,
+              tsb_complete_legendre_elliptic_integral_k_backward_backward)
+TSBH_UNARY_OP(complete_legendre_elliptic_integral_e, CompleteLegendreEllipticIntegralE, m,
+              tsb_complete_legendre_elliptic_integral_e, tsb_complete_legendre_elliptic_integral_e_backward,
+              tsb_complete_legendre_elliptic_integral_e_backward_backward)
+
+// Library-level controls (not part of the reference's namespace).
+namespace tsbh {
+int64_t set_precision_mode(int64_t mode) {
+  TORCH_CHECK(mode == TSB_PRECISION_AUTO || mode == TSB_PRECISION_FP64, "precision mode must be 0 (auto) or 1 (fp64)");
+  return precision_mode().exchange(static_cast<int>(mode));
+}
+int64_t get_precision_mode() { return precision_mode().load(); }
+std::string library_version() { return tsb_version(); }
+}  // namespace tsbh
+
+TORCH_LIBRARY(torchscience_b200, m) {
+  m.def("set_precision_mode(int mode) -> int", &tsbh::set_precision_mode);
+  m.def("get_precision_mode() -> int", &tsbh::get_precision_mode);
+  m.def("version() -> str", &tsbh::library_version);
+}

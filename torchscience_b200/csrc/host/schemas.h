@@ -1,0 +1,85 @@
+// Schema strings of the special-function operators on the accelerated path,
+// identical to the reference's TORCH_LIBRARY(torchscience, ...) block in
+// src/torchscience/csrc/torchscience.cpp (line numbers per group below).
+// Shared by this package's registration and by the oracle's build of the
+// reference's CPU operators, so both expose the same torch.ops.torchscience
+// interface.
+#pragma once
+
+#define TSB_DEFINE_TORCHSCIENCE_SCHEMAS(m)                                                                          \
+  /* torchscience.cpp:813-815 */                                                                                     \
+  (m).def("gamma(Tensor z) -> Tensor");                                                                              \
+  (m).def("gamma_backward(Tensor grad_output, Tensor z) -> Tensor");                                                 \
+  (m).def("gamma_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");                 \
+  /* torchscience.cpp:817-819 */                                                                                     \
+  (m).def("digamma(Tensor z) -> Tensor");                                                                            \
+  (m).def("digamma_backward(Tensor grad_output, Tensor z) -> Tensor");                                               \
+  (m).def("digamma_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");               \
+  /* torchscience.cpp:821-823 */                                                                                     \
+  (m).def("trigamma(Tensor z) -> Tensor");                                                                           \
+  (m).def("trigamma_backward(Tensor grad_output, Tensor z) -> Tensor");                                              \
+  (m).def("trigamma_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");              \
+  /* torchscience.cpp:837-839 */                                                                                     \
+  (m).def("hypergeometric_2_f_1(Tensor a, Tensor b, Tensor c, Tensor z) -> Tensor");                                 \
+  (m).def(                                                                                                           \
+      "hypergeometric_2_f_1_backward(Tensor grad_output, Tensor a, Tensor b, Tensor c, Tensor z) -> (Tensor, Tensor, " \
+      "Tensor, Tensor)");                                                                                            \
+  (m).def(                                                                                                           \
+      "hypergeometric_2_f_1_backward_backward(Tensor gg_a, Tensor gg_b, Tensor gg_c, Tensor gg_z, Tensor "           \
+      "grad_output, Tensor a, Tensor b, Tensor c, Tensor z) -> (Tensor, Tensor, Tensor, Tensor, Tensor)");           \
+  /* torchscience.cpp:849-851 */                                                                                     \
+  (m).def("log_gamma(Tensor z) -> Tensor");                                                                          \
+  (m).def("log_gamma_backward(Tensor grad_output, Tensor z) -> Tensor");                                             \
+  (m).def("log_gamma_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");             \
+  /* torchscience.cpp:853-855 */                                                                                     \
+  (m).def("regularized_gamma_p(Tensor a, Tensor x) -> Tensor");                                                      \
+  (m).def("regularized_gamma_p_backward(Tensor grad, Tensor a, Tensor x) -> (Tensor, Tensor)");                      \
+  (m).def(                                                                                                           \
+      "regularized_gamma_p_backward_backward(Tensor grad_grad_a, Tensor grad_grad_x, Tensor grad, Tensor a, Tensor " \
+      "x) -> (Tensor, Tensor, Tensor)");                                                                             \
+  /* torchscience.cpp:857-859 */                                                                                     \
+  (m).def("regularized_gamma_q(Tensor a, Tensor x) -> Tensor");                                                      \
+  (m).def("regularized_gamma_q_backward(Tensor grad, Tensor a, Tensor x) -> (Tensor, Tensor)");                      \
+  (m).def(                                                                                                           \
+      "regularized_gamma_q_backward_backward(Tensor grad_grad_a, Tensor grad_grad_x, Tensor grad, Tensor a, Tensor " \
+      "x) -> (Tensor, Tensor, Tensor)");                                                                             \
+  /* torchscience.cpp:872-874 */                                                                                     \
+  (m).def("bessel_j_0(Tensor z) -> Tensor");                                                                         \
+  (m).def("bessel_j_0_backward(Tensor grad_output, Tensor z) -> Tensor");                                            \
+  (m).def("bessel_j_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");            \
+  /* torchscience.cpp:902-904 */                                                                                     \
+  (m).def("bessel_j(Tensor n, Tensor z) -> Tensor");                                                                 \
+  (m).def("bessel_j_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                          \
+  (m).def(                                                                                                           \
+      "bessel_j_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> (Tensor, "    \
+      "Tensor, Tensor)");                                                                                            \
+  /* torchscience.cpp:907-909 */                                                                                     \
+  (m).def("bessel_y(Tensor n, Tensor z) -> Tensor");                                                                 \
+  (m).def("bessel_y_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                          \
+  (m).def(                                                                                                           \
+      "bessel_y_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> (Tensor, "    \
+      "Tensor, Tensor)");                                                                                            \
+  /* torchscience.cpp:912-914 */                                                                                     \
+  (m).def("modified_bessel_k(Tensor n, Tensor z) -> Tensor");                                                        \
+  (m).def("modified_bessel_k_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                 \
+  (m).def(                                                                                                           \
+      "modified_bessel_k_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> "    \
+      "(Tensor, Tensor, Tensor)");                                                                                   \
+  /* torchscience.cpp:917-919 */                                                                                     \
+  (m).def("modified_bessel_i(Tensor n, Tensor z) -> Tensor");                                                        \
+  (m).def("modified_bessel_i_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                 \
+  (m).def(                                                                                                           \
+      "modified_bessel_i_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> "    \
+      "(Tensor, Tensor, Tensor)");                                                                                   \
+  /* torchscience.cpp:1015-1017 */                                                                                   \
+  (m).def("complete_legendre_elliptic_integral_k(Tensor m) -> Tensor");                                              \
+  (m).def("complete_legendre_elliptic_integral_k_backward(Tensor grad_output, Tensor m) -> Tensor");                 \
+  (m).def(                                                                                                           \
+      "complete_legendre_elliptic_integral_k_backward_backward(Tensor gg_m, Tensor grad_output, Tensor m) -> "       \
+      "(Tensor, Tensor)");                                                                                           \
+  /* torchscience.cpp:1019-1021 */                                                                                   \
+  (m).def("complete_legendre_elliptic_integral_e(Tensor m) -> Tensor");                                              \
+  (m).def("complete_legendre_elliptic_integral_e_backward(Tensor grad_output, Tensor m) -> Tensor");                 \
+  (m).def(                                                                                                           \
+      "complete_legendre_elliptic_integral_e_backward_backward(Tensor gg_m, Tensor grad_output, Tensor m) -> "       \
+      "(Tensor, Tensor)");

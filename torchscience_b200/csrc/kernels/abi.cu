@@ -1,0 +1,95 @@
+// Library-wide C-ABI helpers: error state, device checks, workspace query.
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <mutex>
+#include <string>
+
+#include "dispatch.cuh"
+
+namespace tsb {
+
+namespace {
+thread_local std::string g_last_error;
+std::mutex g_dev_mutex;
+DeviceInfo g_devices[64];
+bool g_dev_init[64];
+}  // namespace
+
+int32_t set_error(int32_t status, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+int32_t current_device(int* dev, const DeviceInfo** info) {
+  int d = 0;
+  cudaError_t e = cudaGetDevice(&d);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(TSB_ERR_DEVICE, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+  }
+  if (d < 0 || d >= 64) return set_error(TSB_ERR_DEVICE, "device ordinal %d out of range", d);
+  {
+    std::lock_guard<std::mutex> lock(g_dev_mutex);
+    if (!g_dev_init[d]) {
+      DeviceInfo di{};
+      cudaDeviceGetAttribute(&di.sm_count, cudaDevAttrMultiProcessorCount, d);
+      cudaDeviceGetAttribute(&di.major, cudaDevAttrComputeCapabilityMajor, d);
+      cudaDeviceGetAttribute(&di.minor, cudaDevAttrComputeCapabilityMinor, d);
+      e = cudaGetLastError();
+      di.ok = e == cudaSuccess && di.major == 10 && di.minor == 0 && di.sm_count > 0;
+      g_devices[d] = di;
+      g_dev_init[d] = true;
+    }
+  }
+  const DeviceInfo& di = g_devices[d];
+  if (!di.ok)
+    return set_error(TSB_ERR_DEVICE,
+                     "device %d has compute capability %d.%d; these kernels are built for sm_100a (B200, 10.0) only", d,
+                     di.major, di.minor);
+  *dev = d;
+  *info = &di;
+  return TSB_OK;
+}
+
+}  // namespace tsb
+
+extern "C" {
+
+const char* tsb_version(void) { return "torchscience_b200 0.1.0 (sm_100a)"; }
+
+const char* tsb_last_error(void) { return tsb::g_last_error.c_str(); }
+
+const char* tsb_status_string(int32_t status) {
+  switch (status) {
+    case TSB_OK: return "ok";
+    case TSB_ERR_ARGUMENT: return "invalid argument";
+    case TSB_ERR_DTYPE: return "unsupported or mixed dtype";
+    case TSB_ERR_LAYOUT: return "reduced-output layout not supported by the fused kernel";
+    case TSB_ERR_WORKSPACE: return "workspace missing or too small";
+    case TSB_ERR_LAUNCH: return "CUDA launch failure";
+    case TSB_ERR_DEVICE: return "no usable sm_100 device";
+    default: return "unknown status";
+  }
+}
+
+int64_t tsb_workspace_bytes(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_t n_out) {
+  tsb::Canon c;
+  int32_t dtype = 0;
+  const int32_t st = tsb::canonicalize(in, n_in, out, n_out, n_in, n_out, c, dtype);
+  if (st) return st;
+  bool reduced = false;
+  for (int o = 0; o < n_out; ++o)
+    if (out[o].data && tsb::output_is_reduced(c, n_in + o)) reduced = true;
+  if (!reduced) return 0;
+  if (c.ndim > 2)
+    return tsb::set_error(TSB_ERR_LAYOUT, "reduced outputs need an iteration space of at most 2 coalesced dims");
+  return tsb::reduce_ws_bytes(c, n_in, out, n_out, tsb::kTR);
+}
+
+}  // extern "C"

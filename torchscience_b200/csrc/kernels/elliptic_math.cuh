@@ -1,0 +1,168 @@
+// Complete elliptic integrals K(m), E(m) (parameter convention) and their
+// first and second derivatives in m.
+//
+// The reference evaluates K = R_F(0, 1-m, 1) and E = 2 R_G(0, 1-m, 1) by
+// Carlson duplication (complete_legendre_elliptic_integral_k.h:29-33,
+// complete_legendre_elliptic_integral_e.h:71-79) and differentiates E by a
+// central difference with h = 1e-6 (complete_legendre_elliptic_integral_e_backward.h:41-52).
+// Here both come from one arithmetic-geometric mean sweep (DLMF 19.8.1 and
+// 19.8.6): a_{n+1} = (a+b)/2, b_{n+1} = sqrt(ab), c_{n+1} = (a-b)/2 from
+// a_0 = 1, b_0 = sqrt(1-m); K = π/(2 a_N), E = K (1 - Σ 2^(n-1) c_n²) with
+// c_0² = m.  The sweep converges quadratically (≈ 7 steps at m = 1 - 1e-9).
+// Derivatives use the closed forms (DLMF 19.4.1)
+//   dK/dm = (E - (1-m)K) / (2m(1-m)),  dE/dm = (E - K) / (2m)
+// and their m-derivatives; for small |m| these cancel, so there the
+// Maclaurin series K = π/2 Σ c_n m^n, c_n = ((2n-1)!!/(2n)!!)² (DLMF 19.5.1)
+// and its E counterpart are summed instead.
+#pragma once
+
+#include <math_constants.h>
+
+namespace tsb {
+
+template <typename T>
+struct EllipKE {
+  T K, E;      // values
+  T Kp, Ep;    // d/dm
+  T Kpp, Epp;  // d²/dm²
+};
+
+template <typename T>
+__device__ __forceinline__ T sqrt_t(T v);
+template <>
+__device__ __forceinline__ double sqrt_t<double>(double v) { return sqrt(v); }
+template <>
+__device__ __forceinline__ float sqrt_t<float>(float v) { return sqrtf(v); }
+
+// Maclaurin series for |m| small: K, E and derivatives up to ORDER.
+template <typename T, int ORDER, int NTERMS>
+__device__ inline EllipKE<T> ellip_series(T m) {
+  EllipKE<T> r;
+  T c = 1;        // c_n
+  T mp = 1;       // m^n
+  T mp1 = 0;      // m^(n-1)   (n >= 1)
+  T mp2 = 0;      // m^(n-2)   (n >= 2)
+  T K = 1, E = 1, Kp = 0, Ep = 0, Kpp = 0, Epp = 0;
+#pragma unroll
+  for (int n = 1; n <= NTERMS; ++n) {
+    const T f = T(2 * n - 1) / T(2 * n);
+    c *= f * f;
+    mp2 = mp1;
+    mp1 = mp;
+    mp *= m;
+    const T inv = T(1) / T(2 * n - 1);
+    K += c * mp;
+    E -= c * mp * inv;
+    if (ORDER >= 1) {
+      Kp += T(n) * c * mp1;
+      Ep -= T(n) * c * mp1 * inv;
+    }
+    if (ORDER >= 2 && n >= 2) {
+      Kpp += T(n * (n - 1)) * c * mp2;
+      Epp -= T(n * (n - 1)) * c * mp2 * inv;
+    }
+  }
+  const T h = T(CUDART_PIO2);
+  r.K = h * K;
+  r.E = h * E;
+  r.Kp = h * Kp;
+  r.Ep = h * Ep;
+  r.Kpp = h * Kpp;
+  r.Epp = h * Epp;
+  return r;
+}
+
+template <typename T, int ORDER>
+__device__ inline EllipKE<T> ellip_agm(T m) {
+  EllipKE<T> r;
+  const T eps = sizeof(T) == 8 ? T(1e-16) : T(3e-8);
+  T a = 1, b = sqrt_t<T>(T(1) - m);
+  T sum = T(0.5) * m;  // 2^(n-1) c_n², n = 0
+  T pw = T(0.5);
+  for (int it = 0; it < 40; ++it) {
+    const T c = T(0.5) * (a - b);
+    const T an = T(0.5) * (a + b);
+    b = sqrt_t<T>(a * b);
+    a = an;
+    pw *= T(2);
+    sum += pw * c * c;
+    if (fabs(c) <= eps * a) break;
+  }
+  r.K = T(CUDART_PIO2) / a;
+  r.E = r.K * (T(1) - sum);
+  r.Kp = r.Ep = r.Kpp = r.Epp = 0;
+  if (ORDER >= 1) {
+    const T mc = T(1) - m;
+    r.Kp = (r.E - mc * r.K) / (T(2) * m * mc);
+    r.Ep = (r.E - r.K) / (T(2) * m);
+    if (ORDER >= 2) {
+      const T N = r.E - mc * r.K, Dn = T(2) * m * mc;
+      const T Np = r.Ep + r.K - mc * r.Kp, Dnp = T(2) * (T(1) - T(2) * m);
+      r.Kpp = (Np * Dn - N * Dnp) / (Dn * Dn);
+      r.Epp = (r.Ep - r.Kp) / (T(2) * m) - r.Ep / m;
+    }
+  }
+  return r;
+}
+
+// K, E (+ derivatives) with the reference's domain conventions:
+// NaN for m > 1 (sqrt of a negative in R_F), K(1) = +inf, E(1) = 1.
+template <typename T, int ORDER>
+__device__ inline EllipKE<T> ellip_eval(T m) {
+  EllipKE<T> r;
+  const T nan = T(CUDART_NAN), inf = T(CUDART_INF);
+  if (isnan(m) || m > T(1)) {
+    r.K = r.E = r.Kp = r.Ep = r.Kpp = r.Epp = nan;
+    return r;
+  }
+  if (m == T(1)) {
+    r.K = inf;
+    r.E = T(1);
+    r.Kp = inf;
+    r.Ep = -inf;
+    r.Kpp = inf;
+    r.Epp = -inf;
+    return r;
+  }
+  if (isinf(m)) {  // m = -inf
+    r.K = T(0);
+    r.E = inf;
+    r.Kp = T(0);
+    r.Ep = T(0);
+    r.Kpp = T(0);
+    r.Epp = T(0);
+    return r;
+  }
+  const T small = sizeof(T) == 8 ? T(0.1) : T(0.3);
+  if (ORDER >= 1 && fabs(m) < small) return ellip_series<T, ORDER, sizeof(T) == 8 ? 20 : 16>(m);
+  return ellip_agm<T, ORDER>(m);
+}
+
+// Mixed: float AGM except near m = 1, where E = K(1 - Σ) cancels by a factor
+// ~K and the FP64 sweep is used.
+template <int ORDER>
+__device__ inline EllipKE<float> ellip_eval_m(float m) {
+  if (m > 0.9f && m < 1.0f) {
+    const EllipKE<double> d = ellip_eval<double, ORDER>((double)m);
+    EllipKE<float> r;
+    r.K = (float)d.K;
+    r.E = (float)d.E;
+    r.Kp = (float)d.Kp;
+    r.Ep = (float)d.Ep;
+    r.Kpp = (float)d.Kpp;
+    r.Epp = (float)d.Epp;
+    return r;
+  }
+  return ellip_eval<float, ORDER>(m);
+}
+
+template <int ORDER>
+__device__ __forceinline__ EllipKE<double> ellip_t(double m) {
+  return ellip_eval<double, ORDER>(m);
+}
+template <int ORDER>
+__device__ __forceinline__ EllipKE<float> ellip_t(float m) {
+  return ellip_eval_m<ORDER>(m);
+}
+
+}  // namespace tsb

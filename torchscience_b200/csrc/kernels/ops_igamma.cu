@@ -1,0 +1,80 @@
+// Regularized incomplete gamma P(a,x) and Q(a,x) = 1 - P: forward, backward
+// (grad_a, grad_x) and double-backward entry points.  Output conventions
+// follow regularized_gamma_p_backward.h:27-33 and
+// regularized_gamma_p_backward_backward.h:12-41 (Q negates every derivative,
+// regularized_gamma_q_backward_backward.h:16-21).
+#include "dispatch.cuh"
+#include "igamma_math.cuh"
+
+namespace tsb {
+
+// ∂P/∂x alone (backward with grad_a not requested): no series needed.
+__device__ __forceinline__ double igamma_px_only(double a, double x) {
+  if (isnan(a) || isnan(x) || x < 0.0 || a <= 0.0) return CUDART_NAN;
+  if (x == 0.0 || isinf(x) || isinf(a)) return 0.0;
+  return exp(igamma_log_prefix_d(a, x) + log(a / x));
+}
+
+template <typename T_, bool UPPER>
+struct IgammaFwd {
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 1, R = kIgRegions;
+  static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return igamma_classify((double)in[0], (double)in[1]); }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t) {
+    const IgammaOut o = igamma_eval<0>(r, in[0], in[1]);
+    out[0] = (T)(UPPER ? o.q : o.p);
+  }
+};
+
+template <typename T_, bool UPPER>
+struct IgammaBwd {
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = kIgRegions;
+  static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return igamma_classify((double)in[1], (double)in[2]); }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t mask) {
+    const double sgn = UPPER ? -1.0 : 1.0;
+    const double g = in[0];
+    if (!(mask & 1u)) {
+      out[0] = T(0);
+      out[1] = (T)(sgn * g * igamma_px_only((double)in[1], (double)in[2]));
+      return;
+    }
+    const IgammaOut o = igamma_eval<1>(r, in[1], in[2]);
+    out[0] = (T)(sgn * g * o.pa);
+    out[1] = (T)(sgn * g * o.px);
+  }
+};
+
+template <typename T_, bool UPPER>
+struct IgammaBwdBwd {
+  using T = T_;
+  static constexpr int NIN = 5, NOUT = 3, R = kIgRegions;
+  static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return igamma_classify((double)in[3], (double)in[4]); }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t) {
+    const double sgn = UPPER ? -1.0 : 1.0;
+    const double gga = in[0], ggx = in[1], g = in[2];
+    const IgammaOut o = igamma_eval<2>(r, in[3], in[4]);
+    out[0] = (T)(sgn * (gga * o.pa + ggx * o.px));
+    out[1] = (T)(sgn * g * (gga * o.paa + ggx * o.pax));
+    out[2] = (T)(sgn * g * (gga * o.pax + ggx * o.pxx));
+  }
+};
+
+template <typename T> using GammaPFwd = IgammaFwd<T, false>;
+template <typename T> using GammaPBwd = IgammaBwd<T, false>;
+template <typename T> using GammaPBwdBwd = IgammaBwdBwd<T, false>;
+template <typename T> using GammaQFwd = IgammaFwd<T, true>;
+template <typename T> using GammaQBwd = IgammaBwd<T, true>;
+template <typename T> using GammaQBwdBwd = IgammaBwdBwd<T, true>;
+
+}  // namespace tsb
+
+TSB_DEFINE_OP(tsb_regularized_gamma_p, tsb::GammaPFwd)
+TSB_DEFINE_OP(tsb_regularized_gamma_p_backward, tsb::GammaPBwd)
+TSB_DEFINE_OP(tsb_regularized_gamma_p_backward_backward, tsb::GammaPBwdBwd)
+TSB_DEFINE_OP(tsb_regularized_gamma_q, tsb::GammaQFwd)
+TSB_DEFINE_OP(tsb_regularized_gamma_q_backward, tsb::GammaQBwd)
+TSB_DEFINE_OP(tsb_regularized_gamma_q_backward_backward, tsb::GammaQBwdBwd)
