@@ -81,8 +81,9 @@ def igamma():
         d[f"ref_{nm}"] = ref(nm, 0, a, x)[0]
         ga, gx = ref(nm, 1, g, a, x)
         d[f"ref_{nm}_grad_a"], d[f"ref_{nm}_grad_x"] = ga, gx
-    d["truth_p"] = sp.gammainc(a, x)
-    d["truth_q"] = sp.gammaincc(a, x)
+    # mpmath at 40 digits: scipy's gammainc is only good to ~1e-12 at large a.
+    d["truth_p"] = np.array([float(mp.gammainc(mp.mpf(ai), 0, mp.mpf(xi), regularized=True)) if ai > 0 and xi > 0 else sp.gammainc(ai, xi) for ai, xi in zip(a, x)])
+    d["truth_q"] = np.array([float(mp.gammainc(mp.mpf(ai), mp.mpf(xi), mp.inf, regularized=True)) if ai > 0 and xi > 0 else sp.gammaincc(ai, xi) for ai, xi in zip(a, x)])
     # Derivatives from mpmath at 40 digits on a subsample.
     idx = rng.choice(a.size - 5, 160, replace=False)
     d["deriv_idx"] = idx
@@ -93,9 +94,16 @@ def igamma():
         def P(aa, xx):
             return mp.gammainc(aa, 0, xx, regularized=True)
 
-        pa.append(float(mp.diff(lambda t: P(t, xi), ai)))
+        def Q(aa, xx):
+            return mp.gammainc(aa, xx, mp.inf, regularized=True)
+
+        # Differentiate whichever of P, Q is small: the other is 1 - tiny and a
+        # numerical derivative of it would lose the digits that matter.
+        upper = xi > ai
+        f = (lambda t: -Q(t, xi)) if upper else (lambda t: P(t, xi))
+        pa.append(float(mp.diff(f, ai)))
         px.append(float(mp.exp((ai - 1) * mp.log(xi) - xi - mp.loggamma(ai))))
-        paa.append(float(mp.diff(lambda t: P(t, xi), ai, 2)))
+        paa.append(float(mp.diff(f, ai, 2)))
         pax.append(float(mp.diff(lambda t: mp.exp((t - 1) * mp.log(xi) - xi - mp.loggamma(t)), ai)))
         pxx.append(float(px[-1] * ((ai - 1) / xi - 1)))
     d["truth_pa"], d["truth_px"] = np.array(pa), np.array(px)

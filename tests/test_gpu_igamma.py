@@ -19,19 +19,21 @@ def cuda(a, dtype=torch.float64):
     return torch.tensor(np.asarray(a), dtype=dtype, device="cuda")
 
 
-def test_fp64_values_against_scipy():
+def test_fp64_values_against_mpmath():
+    """Relative error within 8 ulp x (1 + |ln value|) + 2e-14: the exponent
+    a ln x - x - lnΓ(a) carries an absolute rounding error proportional to its
+    size, which no double evaluation avoids (values down to e^-700 occur here);
+    the 2e-14 floor covers the a < 10 branch, where the exponent is formed
+    from terms of size ~20 directly."""
     (p,) = run("regularized_gamma_p", cuda(A), cuda(X))
     (q,) = run("regularized_gamma_q", cuda(A), cuda(X))
     p, q = p.cpu().numpy(), q.cpu().numpy()
-    tp, tq = D["truth_p"], D["truth_q"]
-    mp_ = tp > 1e-290
-    mq = tq > 1e-290
-    ep = rel_err(p, tp)[mp_]
-    eq = rel_err(q, tq)[mq]
-    assert ep.max() <= 1e-12, f"P max rel err {ep.max():.3e}"
-    # Q = 1 - P in the series region loses digits only when P -> 1 (small a); cap at 1e-10
-    assert eq.max() <= 1e-10, f"Q max rel err {eq.max():.3e}"
-    assert np.all(np.abs(p + q - 1) <= 4e-16)
+    for got, tru in ((p, D["truth_p"]), (q, D["truth_q"])):
+        m = tru > 1e-300
+        bound = 8 * 2.2e-16 * (1 + np.abs(np.log(tru[m]))) + 2e-14
+        e = rel_err(got, tru)[m]
+        assert np.all(e <= bound), f"max rel err {e.max():.3e}, worst ratio {np.max(e / bound):.2f}"
+    assert np.all(np.abs(p + q - 1) <= 8e-16)
 
 
 def test_fp64_parity_with_reference():

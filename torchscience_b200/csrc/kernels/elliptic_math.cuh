@@ -75,7 +75,11 @@ __device__ inline EllipKE<T> ellip_series(T m) {
 template <typename T, int ORDER>
 __device__ inline EllipKE<T> ellip_agm(T m) {
   EllipKE<T> r;
-  const T eps = sizeof(T) == 8 ? T(1e-16) : T(3e-8);
+  // Stop once c_{n+1} <= tol·a_{n+1} with tol ~ sqrt(eps): convergence is
+  // quadratic, so the next c would be ~tol²/4·a, below the working precision,
+  // and a_{n+1} already equals the mean to within it.  (A test against eps
+  // itself can stall with a, b one ulp apart.)
+  const T tol = sizeof(T) == 8 ? T(1e-8) : T(2.4e-4);
   T a = 1, b = sqrt_t<T>(T(1) - m);
   T sum = T(0.5) * m;  // 2^(n-1) c_n², n = 0
   T pw = T(0.5);
@@ -86,7 +90,7 @@ __device__ inline EllipKE<T> ellip_agm(T m) {
     a = an;
     pw *= T(2);
     sum += pw * c * c;
-    if (fabs(c) <= eps * a) break;
+    if (fabs(c) <= tol * a) break;
   }
   r.K = T(CUDART_PIO2) / a;
   r.E = r.K * (T(1) - sum);

@@ -5,17 +5,23 @@
 //   - lnΓ and Γ: CUDA's lgamma/tgamma (called, not re-implemented), with
 //     the reference's conventions at the poles (log_gamma.h:40-46: +inf at
 //     the non-positive integers; gamma.h:84-87: +inf there as well).
-//   - ψ^(n), n = 0..3: recurrence ψ^(n)(x) = ψ^(n)(x+1) - (-1)^n n!/x^(n+1)
-//     up to x >= X0, then the Bernoulli asymptotic series (DLMF 5.15.8,
-//     5.11.2); for x <= 0 the reflection formulas (DLMF 5.5.4, 5.15.6).  The
-//     shifted sums are accumulated as one fraction num/den so the recurrence
-//     costs a single division.
+//   - ψ^(n), n = 1..3: recurrence ψ^(n)(x) = ψ^(n)(x+1) - (-1)^n n!/x^(n+1)
+//     up to a threshold, then the Bernoulli asymptotic series (DLMF 5.15.8,
+//     5.11.2); for x <= 0 the reflection formulas (DLMF 5.15.6).  The shifted
+//     sums are accumulated as one fraction num/den so the recurrence costs a
+//     single division.
+//   - ψ: the same asymptotic series for x >= 10 (8 in FP32); on [1, 2) the
+//     factored fit (x - x0)·P(2x - 3) around the positive root x0 (fits.cuh,
+//     generated by fits/gen_fits.py); other x reach [1, 2) by the recurrence;
+//     reflection (DLMF 5.5.4) for x <= 0.
 // The reference's own digamma/trigamma (digamma.h:10-25, trigamma.h:10-25)
 // use a 3-term asymptotic after shifting to 6; their truncation error is
 // about 1e-8, which the longer series here removes.
 #pragma once
 
 #include <math_constants.h>
+
+#include "fits.cuh"
 
 namespace tsb {
 
@@ -41,8 +47,20 @@ __device__ __forceinline__ double gamma_d(double x) {
   return tgamma(x);
 }
 
+template <typename T, int N>
+__device__ __forceinline__ T horner(const T (&c)[N], T u) {
+  T r = c[N - 1];
+#pragma unroll
+  for (int k = N - 2; k >= 0; --k) r = fma(r, u, c[k]);
+  return r;
+}
+
 // ψ(x).  At the non-positive integers: -inf (the reference's upward
-// recurrence divides by zero there, digamma.h:16-19).
+// recurrence divides by zero there, digamma.h:16-19).  On [1, 2) ψ is
+// evaluated as (x - x0)·P(2x - 3) with x0 the positive root and P a fitted
+// polynomial (fits.cuh), so it keeps full relative accuracy through the root;
+// other x < 10 reach [1, 2) by the recurrence (one step up from (0, 1), or
+// down from [2, 10) as a single fraction), x >= 10 uses the asymptotic series.
 __device__ inline double digamma_d(double x) {
   if (isnan(x)) return x;
   if (isinf(x)) return x > 0.0 ? x : CUDART_NAN;
@@ -54,16 +72,27 @@ __device__ inline double digamma_d(double x) {
     refl = -CUDART_PI * c / s;  // ψ(x) = ψ(1-x) - π cot(πx)
     x = 1.0 - x;
   }
-  double num = 0.0, den = 1.0;  // Σ 1/(x+k) as num/den
-  while (x < 10.0) {
-    num = fma(num, x, den);
-    den *= x;
-    x += 1.0;
+  if (x >= 10.0) {
+    const double z = 1.0 / (x * x);
+    const double tail =
+        z * (TSB_B2 / 2 + z * (TSB_B4 / 4 + z * (TSB_B6 / 6 + z * (TSB_B8 / 8 + z * (TSB_B10 / 10 + z * (TSB_B12 / 12 + z * (TSB_B14 / 14 + z * (TSB_B16 / 16))))))));
+    return refl + ((log(x) - 0.5 / x) - tail);
   }
-  const double z = 1.0 / (x * x);
-  const double tail =
-      z * (TSB_B2 / 2 + z * (TSB_B4 / 4 + z * (TSB_B6 / 6 + z * (TSB_B8 / 8 + z * (TSB_B10 / 10 + z * (TSB_B12 / 12 + z * (TSB_B14 / 14 + z * (TSB_B16 / 16))))))));
-  return refl + ((log(x) - 0.5 / x) - tail) - num / den;
+  double acc = 0.0;
+  if (x < 1.0) {
+    acc = -1.0 / x;  // ψ(x) = ψ(x+1) - 1/x
+    x += 1.0;
+  } else if (x >= 2.0) {
+    double num = 0.0, den = 1.0;  // ψ(x) = ψ(x-n) + Σ_{k=1..n} 1/(x-k)
+    while (x >= 2.0) {
+      x -= 1.0;
+      num = fma(num, x, den);
+      den *= x;
+    }
+    acc = num / den;
+  }
+  const double r = ((x - fits::PSI_X0_HI) - fits::PSI_X0_LO) * horner(fits::PSI_ROOT_D, fma(2.0, x, -3.0));
+  return refl + (r + acc);
 }
 
 // ψ'(x).  +inf at the non-positive integers (trigamma.h:16-19 divides by 0).
@@ -151,10 +180,12 @@ __device__ inline double pentagamma_d(double x) {
 }
 
 // ------------------------------------------------------------------ mixed
-// FP32 bulk; x <= 0 (reflection, cancellation near the negative roots) and the
-// band around ψ's positive root x0 = 1.4616... go to the FP64 evaluators.
+// FP32 evaluators.  Arguments whose FP32 evaluation would lose accuracy
+// (x <= 0: reflection and the negative roots; lnΓ near its zeros at 1 and 2)
+// are classified into an FP64 region by the kernels in ops_gamma.cu; the
+// guards here only keep the functions total when called directly.
 __device__ __forceinline__ float lgamma_m(float x) {
-  if (x <= 0.0f || (x > 0.5f && x < 3.0f)) return (float)lgamma_d((double)x);
+  if (x <= 0.0f) return (float)lgamma_d((double)x);
   return lgammaf(x);
 }
 
@@ -164,17 +195,28 @@ __device__ __forceinline__ float gamma_m(float x) {
 }
 
 __device__ inline float digamma_m(float x) {
-  if (!(x > 0.0f) || fabsf(x - 1.4616321f) < 0.3f) return (float)digamma_d((double)x);
+  if (!(x > 0.0f)) return (float)digamma_d((double)x);
   if (isinf(x)) return x;
-  float num = 0.0f, den = 1.0f;
-  while (x < 8.0f) {
-    num = fmaf(num, x, den);
-    den *= x;
-    x += 1.0f;
+  if (x >= 8.0f) {
+    const float z = 1.0f / (x * x);
+    const float tail = z * ((float)(TSB_B2 / 2) + z * ((float)(TSB_B4 / 4) + z * ((float)(TSB_B6 / 6) + z * (float)(TSB_B8 / 8))));
+    return (logf(x) - 0.5f / x) - tail;
   }
-  const float z = 1.0f / (x * x);
-  const float tail = z * ((float)(TSB_B2 / 2) + z * ((float)(TSB_B4 / 4) + z * ((float)(TSB_B6 / 6) + z * (float)(TSB_B8 / 8))));
-  return ((logf(x) - 0.5f / x) - tail) - num / den;
+  float acc = 0.0f;
+  if (x < 1.0f) {
+    acc = -1.0f / x;
+    x += 1.0f;
+  } else if (x >= 2.0f) {
+    float num = 0.0f, den = 1.0f;
+    while (x >= 2.0f) {
+      x -= 1.0f;
+      num = fmaf(num, x, den);
+      den *= x;
+    }
+    acc = num / den;
+  }
+  const float r = ((x - fits::PSI_X0_HI_F) - fits::PSI_X0_LO_F) * horner(fits::PSI_ROOT_F, fmaf(2.0f, x, -3.0f));
+  return r + acc;
 }
 
 __device__ inline float trigamma_m(float x) {

@@ -21,6 +21,7 @@
 
 #include <math_constants.h>
 
+#include "fits.cuh"
 #include "gamma_math.cuh"
 
 namespace tsb {
@@ -29,13 +30,15 @@ constexpr int kIgammaMaxIter = 2000;
 
 template <typename T>
 struct IgammaEps;
+// Stopping tolerances: 2 ulp, so that convergents that jitter in the last
+// bit (FMA contraction) still terminate.
 template <>
 struct IgammaEps<double> {
-  static constexpr double v = 1.1102230246251565e-16;
+  static constexpr double v = 4.440892098500626e-16;
 };
 template <>
 struct IgammaEps<float> {
-  static constexpr float v = 5.9604645e-08f;
+  static constexpr float v = 2.3841858e-07f;
 };
 
 // log(1+t) - t, accurate for all t > -1.
@@ -58,10 +61,14 @@ __device__ inline double stirling_mu_d(double a) {
 }
 
 // ln D(a,x), D = x^a e^{-x} / Γ(a+1).
+// For a >= 10 the Temme form a·log1pmx(t) is used near x ~ a (|t| < 1/2);
+// farther out log(x/a) is formed directly so that 1 + t = x/a does not lose
+// the digits that t = (x-a)/a rounds away when x << a.
 __device__ inline double igamma_log_prefix_d(double a, double x) {
   if (a < 10.0) return a * log(x) - x - lgamma(a + 1.0);
   const double t = (x - a) / a;
-  return a * log1pmx_d(t) - 0.5 * log(2.0 * CUDART_PI * a) - stirling_mu_d(a);
+  const double core = fabs(t) < 0.5 ? a * log1pmx_d(t) : a * log(x / a) - (x - a);
+  return core - 0.5 * log(2.0 * CUDART_PI * a) - stirling_mu_d(a);
 }
 
 // Cheap float estimate of ln D used only to classify elements.
@@ -71,25 +78,43 @@ __device__ __forceinline__ float igamma_log_prefix_est(float a, float x) {
 
 // Series S = Σ_{n>=0} x^n / ((a+1)...(a+n)) and its a-derivatives.
 // ORDER 0: S; 1: + S1 = dS/da; 2: + S2 = d²S/da².
+// Terms are produced four at a time from one reciprocal of
+// (a+n+1)(a+n+2)(a+n+3)(a+n+4), which also yields the four 1/(a+n+k) that
+// the harmonic sums H_n = Σ 1/(a+k), H2_n = Σ 1/(a+k)² need
+// (dt_n/da = -t_n H_n, d²t_n/da² = t_n (H_n² + H2_n)).  Only used for
+// x < a + 1, where the terms decrease monotonically.
 template <typename TL, int ORDER>
 __device__ inline void igamma_series(TL a, TL x, TL& S, TL& S1, TL& S2) {
   const TL eps = IgammaEps<TL>::v;
+  const TL x2 = x * x;
   TL term = 1, sum = 1, H = 0, H2 = 0, s1 = 0, s2 = 0;
-  for (int n = 1; n < kIgammaMaxIter; ++n) {
-    const TL r = TL(1) / (a + TL(n));
-    term *= x * r;
-    sum += term;
+  TL e = a;
+  for (int it = 0; it < kIgammaMaxIter / 4; ++it) {
+    const TL e1 = e + TL(1), e2 = e + TL(2), e3 = e + TL(3), e4 = e + TL(4);
+    e = e4;
+    const TL p12 = e1 * e2, p34 = e3 * e4;
+    const TL r = TL(1) / (p12 * p34);
+    const TL tr = term * r;
+    const TL t1 = tr * x * (e2 * p34);
+    const TL t2 = tr * x2 * p34;
+    const TL t3 = tr * (x2 * x) * e4;
+    const TL t4 = tr * (x2 * x2);
+    sum += (t1 + t2) + (t3 + t4);
+    term = t4;
+    bool done = t4 <= eps * sum;
     if (ORDER >= 1) {
-      H += r;
-      s1 -= term * H;
+      const TL r1 = r * (e2 * p34), r2 = r * (e1 * p34), r3 = r * (p12 * e4), r4 = r * (p12 * e3);
+      const TL h1 = H + r1, h2 = h1 + r2, h3 = h2 + r3, h4 = h3 + r4;
+      s1 -= (t1 * h1 + t2 * h2) + (t3 * h3 + t4 * h4);
+      if (ORDER >= 2) {
+        const TL q1 = H2 + r1 * r1, q2 = q1 + r2 * r2, q3 = q2 + r3 * r3, q4 = q3 + r4 * r4;
+        s2 += (t1 * (h1 * h1 + q1) + t2 * (h2 * h2 + q2)) + (t3 * (h3 * h3 + q3) + t4 * (h4 * h4 + q4));
+        H2 = q4;
+        done = done && t4 * (h4 * h4 + q4) <= eps * s2;
+      }
+      H = h4;
+      done = done && t4 * h4 <= eps * fabs(s1);
     }
-    if (ORDER >= 2) {
-      H2 += r * r;
-      s2 += term * (H * H + H2);
-    }
-    bool done = term <= eps * sum;
-    if (ORDER >= 1) done = done && term * H <= eps * fabs(s1);
-    if (ORDER >= 2) done = done && term * (H * H + H2) <= eps * s2;
     if (done) break;
   }
   S = sum;
@@ -99,59 +124,80 @@ __device__ inline void igamma_series(TL a, TL x, TL& S, TL& S1, TL& S2) {
 
 // Continued fraction G = b0 + a1/(b1 + a2/(b2 + ...)), b_n = x + 2n + 1 - a,
 // a_n = -n(n - a), so that Q = x^a e^{-x}/Γ(a) / G.  Returns F = 1/G and its
-// a-derivatives F1, F2 (ORDER as above).
+// a-derivatives F1, F2 (ORDER as above).  The Wallis recurrences
+//   A_n = b_n A_{n-1} + a_n A_{n-2}  (same for B)
+// and their a-derivatives (b_n' = -1, a_n' = n) advance four steps between
+// renormalisations by 1/B_n, which also give the convergent G_n = A_n / B_n.
 template <typename TL, int ORDER>
 __device__ inline void igamma_cf(TL a, TL x, TL& F, TL& F1, TL& F2) {
   const TL eps = IgammaEps<TL>::v;
   const TL b0 = x + TL(1) - a;
-  // Wallis recurrence state: A_{n-1}, A_n (and derivatives), B likewise.
   TL Ap = 1, A = b0, Bp = 0, B = 1;
   TL dAp = 0, dA = -1, dBp = 0, dB = 0;
   TL ddAp = 0, ddA = 0, ddBp = 0, ddB = 0;
   TL G = b0, dG = -1, ddG = 0;
-  for (int n = 1; n < kIgammaMaxIter; ++n) {
-    const TL fn = TL(n);
-    const TL an = -fn * (fn - a);
-    const TL bn = b0 + TL(2) * fn;
-    const TL An = bn * A + an * Ap;
-    const TL Bn = bn * B + an * Bp;
-    TL dAn = 0, dBn = 0, ddAn = 0, ddBn = 0;
-    if (ORDER >= 1) {
-      dAn = bn * dA - A + an * dAp + fn * Ap;
-      dBn = bn * dB - B + an * dBp + fn * Bp;
+  int n = 0;
+  for (int it = 0; it < kIgammaMaxIter / 4; ++it) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      ++n;
+      const TL fn = TL(n);
+      const TL an = -fn * (fn - a);
+      const TL bn = b0 + TL(2) * fn;
+      const TL An = bn * A + an * Ap;
+      const TL Bn = bn * B + an * Bp;
+      if (ORDER >= 2) {
+        const TL ddAn = bn * ddA - TL(2) * dA + an * ddAp + TL(2) * fn * dAp;
+        const TL ddBn = bn * ddB - TL(2) * dB + an * ddBp + TL(2) * fn * dBp;
+        ddAp = ddA;
+        ddA = ddAn;
+        ddBp = ddB;
+        ddB = ddBn;
+      }
+      if (ORDER >= 1) {
+        const TL dAn = bn * dA - A + an * dAp + fn * Ap;
+        const TL dBn = bn * dB - B + an * dBp + fn * Bp;
+        dAp = dA;
+        dA = dAn;
+        dBp = dB;
+        dB = dBn;
+      }
+      Ap = A;
+      A = An;
+      Bp = B;
+      B = Bn;
     }
-    if (ORDER >= 2) {
-      ddAn = bn * ddA - TL(2) * dA + an * ddAp + TL(2) * fn * dAp;
-      ddBn = bn * ddB - TL(2) * dB + an * ddBp + TL(2) * fn * dBp;
-    }
-    const TL s = TL(1) / Bn;
-    Ap = A * s;
-    Bp = B * s;
-    A = An * s;
+    const TL s = TL(1) / B;
+    Ap *= s;
+    Bp *= s;
+    A *= s;
     B = TL(1);
     if (ORDER >= 1) {
-      dAp = dA * s;
-      dBp = dB * s;
-      dA = dAn * s;
-      dB = dBn * s;
+      dAp *= s;
+      dBp *= s;
+      dA *= s;
+      dB *= s;
     }
     if (ORDER >= 2) {
-      ddAp = ddA * s;
-      ddBp = ddB * s;
-      ddA = ddAn * s;
-      ddB = ddBn * s;
+      ddAp *= s;
+      ddBp *= s;
+      ddA *= s;
+      ddB *= s;
     }
+    // Convergence of each quantity is judged against the size of the terms it
+    // is formed from (dG = dA - A·dB can cancel, leaving rounding noise far
+    // above 2 ulp of the result).
     const TL Gn = A;
     bool done = fabs(Gn - G) <= eps * fabs(Gn);
     G = Gn;
     if (ORDER >= 1) {
       const TL dGn = dA - A * dB;
-      done = done && fabs(dGn - dG) <= eps * fabs(dGn);
+      done = done && fabs(dGn - dG) <= eps * (fabs(dA) + fabs(A * dB));
       dG = dGn;
     }
     if (ORDER >= 2) {
       const TL ddGn = ddA - TL(2) * dA * dB - A * ddB + TL(2) * A * dB * dB;
-      done = done && fabs(ddGn - ddG) <= eps * fabs(ddGn);
+      done = done && fabs(ddGn - ddG) <= eps * (fabs(ddA) + fabs(TL(2) * dA * dB) + fabs(A * ddB) + fabs(TL(2) * A * dB * dB));
       ddG = ddGn;
     }
     if (done) break;
@@ -175,7 +221,10 @@ enum IgammaRegion : int {
   kIgSeriesHeavy = 2,
   kIgCfLight = 3,
   kIgCfHeavy = 4,
-  kIgRegions = 5
+  kIgSmallA = 5,  // a < 1, x < a + 1: series for P, dedicated formula for Q
+  kIgSat0 = 6,    // P and every derivative underflow to 0 (Q = 1)
+  kIgSat1 = 7,    // Q and every derivative underflow to 0 (P = 1)
+  kIgRegions = 8
 };
 
 // Region of (a, x) from cheap float arithmetic.
@@ -184,18 +233,42 @@ __device__ __forceinline__ int igamma_classify(double ad, double xd) {
   const float a = (float)ad, x = (float)xd;
   if (!(a > 0.0f) || !(x > 0.0f) || isinf(a) || isinf(x)) return kIgSpecial;
   const float lnd = igamma_log_prefix_est(a, x);
+  // Saturation: the prefactor (and ∂P/∂x = D·a/x, whose ratio a/x is
+  // included) is below e^-760, so in double P or Q and all derivatives are 0.
+  // The float estimate is good to far better than the 15-unit margin to the
+  // double underflow threshold e^-745.
+  const float lratio = fmaxf(0.0f, __logf(a / x));
   if (x < a + 1.0f) {
-    // P <= D·(a+1)/(a+1-x) ~ D·a; P underflows below ~e^-750.
-    if (lnd + __logf(a + 1.0f) < -760.0f) return kIgSpecial;
+    // P <= D·(a+1)/(a+1-x) ~ D·a.
+    if (lnd + __logf(a + 1.0f) + lratio < -760.0f) return kIgSat0;
+    if (a < 1.0f) return kIgSmallA;
     return (x < 0.5f * (a + 1.0f)) ? kIgSeriesLight : kIgSeriesHeavy;
   }
   // Q = a D F with F <= 1/(x+1-a) <= 1.
-  if (lnd + __logf(a) < -760.0f) return kIgSpecial;
+  if (lnd + __logf(a) + lratio < -760.0f) return kIgSat1;
   return (x > 2.0f * (a + 1.0f) + 10.0f) ? kIgCfLight : kIgCfHeavy;
 }
 
+// Q(a, x) for a < 1, x < a + 1 without the 1 - P cancellation (P -> 1 as
+// a -> 0): from γ(a,x) = Σ (-1)^n x^(a+n) / (n!(a+n)),
+//   Q = -expm1(a ln x - lnΓ(1+a)) - x^a/Γ(1+a) · a · Σ_{n>=1} (-x)^n / (n!(a+n)),
+// with lnΓ(1+a) = a·G(2a-1) from the fit in fits.cuh (no rounding of 1 + a).
+__device__ inline double igamma_q_small_a_d(double a, double x) {
+  const double lg1p = a * horner(fits::LGAMMA1P_D, fma(2.0, a, -1.0));
+  const double e = a * log(x) - lg1p;
+  double term = 1.0, T = 0.0;
+  for (int n = 1; n < 80; ++n) {
+    term *= -x / (double)n;
+    const double t = term / (a + (double)n);
+    T += t;
+    if (fabs(t) <= 1e-17 * fabs(T)) break;
+  }
+  return -expm1(e) - exp(e) * a * T;
+}
+
 // FP64 evaluation.  ORDER 0: p,q; 1: + pa, px; 2: + paa, pax, pxx.
-template <int ORDER>
+// WANT_Q: Q is requested (selects the small-a formula for Q where it matters).
+template <int ORDER, bool WANT_Q = false>
 __device__ inline IgammaOut igamma_eval_d(double a, double x) {
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
@@ -236,7 +309,7 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x) {
     igamma_series<double, ORDER>(a, x, S, S1, S2);
     const double D = exp(lnD);
     o.p = D * S;
-    o.q = 1.0 - o.p;
+    o.q = (WANT_Q && a < 1.0) ? igamma_q_small_a_d(a, x) : 1.0 - o.p;
     if (ORDER >= 1) {
       const double L1 = lx - (psi_a + 1.0 / a);  // d lnD/da = ln x - ψ(a+1)
       o.pa = D * fma(L1, S, S1);
@@ -281,8 +354,12 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x) {
 // float for the light regions, everything in double for the heavy regions
 // (large a near the transition x ~ a, where the term count grows like √a and
 // float accumulation would exceed 1e-6).
-template <int ORDER>
+template <int ORDER, bool WANT_Q = false>
 __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf) {
+  if (region == kIgSmallA) {
+    if (WANT_Q) return igamma_eval_d<ORDER, true>((double)af, (double)xf);
+    region = kIgSeriesLight;
+  }
   if (region != kIgSeriesLight && region != kIgCfLight) return igamma_eval_d<ORDER>((double)af, (double)xf);
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
@@ -334,13 +411,23 @@ __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf) {
   return o;
 }
 
-template <int ORDER>
-__device__ __forceinline__ IgammaOut igamma_eval(int region, double a, double x) {
-  return igamma_eval_d<ORDER>(a, x);
+__device__ __forceinline__ IgammaOut igamma_saturated(bool upper_is_zero) {
+  IgammaOut o;
+  o.p = upper_is_zero ? 1.0 : 0.0;
+  o.q = 1.0 - o.p;
+  o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
+  return o;
 }
-template <int ORDER>
+
+template <int ORDER, bool WANT_Q = false>
+__device__ __forceinline__ IgammaOut igamma_eval(int region, double a, double x) {
+  if (region == kIgSat0 || region == kIgSat1) return igamma_saturated(region == kIgSat1);
+  return igamma_eval_d<ORDER, WANT_Q>(a, x);
+}
+template <int ORDER, bool WANT_Q = false>
 __device__ __forceinline__ IgammaOut igamma_eval(int region, float a, float x) {
-  return igamma_eval_m<ORDER>(region, a, x);
+  if (region == kIgSat0 || region == kIgSat1) return igamma_saturated(region == kIgSat1);
+  return igamma_eval_m<ORDER, WANT_Q>(region, a, x);
 }
 
 }  // namespace tsb

@@ -22,7 +22,7 @@ struct IgammaFwd {
   static constexpr bool REDUCE = false;
   __device__ static int classify(const T* in) { return igamma_classify((double)in[0], (double)in[1]); }
   __device__ static void eval(int r, const T* in, T* out, uint32_t) {
-    const IgammaOut o = igamma_eval<0>(r, in[0], in[1]);
+    const IgammaOut o = igamma_eval<0, UPPER>(r, in[0], in[1]);
     out[0] = (T)(UPPER ? o.q : o.p);
   }
 };
