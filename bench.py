@@ -151,16 +151,18 @@ def timed_steps(fn, steps, warmup, flush):
 
 
 def count_launches(fn) -> int:
-    from torch.profiler import ProfilerActivity, profile
+    """Kernels of this library (names in namespace tsb::) launched by one step,
+    counted with the torch profiler (-1 if the profiler is unavailable, e.g.
+    under an external profiler)."""
+    try:
+        from torch.profiler import ProfilerActivity, profile
 
-    with profile(activities=[ProfilerActivity.CUDA]) as prof:
-        fn()
-        torch.cuda.synchronize()
-    n = 0
-    for ev in prof.events():
-        if ev.device_type == torch.autograd.DeviceType.CUDA and ("tsb" in ev.name):
-            n += 1
-    return n
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        return sum(1 for ev in prof.events() if ev.device_type == torch.autograd.DeviceType.CUDA and "tsb" in ev.name)
+    except Exception:
+        return -1
 
 
 def kernel_roofline(dev_inputs, steps, flush):

@@ -9,6 +9,10 @@
 // 19.8.6): a_{n+1} = (a+b)/2, b_{n+1} = sqrt(ab), c_{n+1} = (a-b)/2 from
 // a_0 = 1, b_0 = sqrt(1-m); K = π/(2 a_N), E = K (1 - Σ 2^(n-1) c_n²) with
 // c_0² = m.  The sweep converges quadratically (≈ 7 steps at m = 1 - 1e-9).
+// For m > 0.9 the values come instead from the complementary-parameter
+// expansions in m1 = 1 - m (DLMF 19.12.1, 19.12.2), which carry the
+// logarithmic singularity explicitly and avoid E = K(1 - Σ) cancelling by a
+// factor ~K near m = 1.
 // Derivatives use the closed forms (DLMF 19.4.1)
 //   dK/dm = (E - (1-m)K) / (2m(1-m)),  dE/dm = (E - K) / (2m)
 // and their m-derivatives; for small |m| these cancel, so there the
@@ -72,6 +76,34 @@ __device__ inline EllipKE<T> ellip_series(T m) {
   return r;
 }
 
+template <typename T>
+__device__ __forceinline__ T log_t(T v);
+template <>
+__device__ __forceinline__ double log_t<double>(double v) { return log(v); }
+template <>
+__device__ __forceinline__ float log_t<float>(float v) { return logf(v); }
+
+// K(m), E(m) for m1 = 1 - m small (m1 < 0.1):
+//   K = Σ c_n m1^n (L + d_n),  E = 1 + (m1/2) Σ e_n m1^n (L + d_n - 1/((2n+1)(2n+2)))
+// with L = -ln(m1)/2, c_n = ((1/2)_n/n!)², e_n = (1/2)_n (3/2)_n / ((2)_n n!),
+// d_0 = ln 4, d_n = d_{n-1} - 2/((2n-1)(2n)).
+template <typename T, int NTERMS>
+__device__ inline void ellip_comp_series(T m1, T& K, T& E) {
+  const T L = T(-0.5) * log_t<T>(m1);
+  T c = 1, ce = 1, d = T(1.3862943611198906), p = 1, k = 0, e = 0;
+#pragma unroll
+  for (int n = 0; n < NTERMS; ++n) {
+    k += c * p * (L + d);
+    e += ce * p * (L + d - T(1) / T((2 * n + 1) * (2 * n + 2)));
+    c *= (T(2 * n + 1) / T(2 * n + 2)) * (T(2 * n + 1) / T(2 * n + 2));
+    ce *= T((2 * n + 1) * (2 * n + 3)) / T(4 * (n + 2) * (n + 1));
+    d -= T(2) / T((2 * n + 1) * (2 * n + 2));
+    p *= m1;
+  }
+  K = k;
+  E = T(1) + T(0.5) * m1 * e;
+}
+
 template <typename T, int ORDER>
 __device__ inline EllipKE<T> ellip_agm(T m) {
   EllipKE<T> r;
@@ -83,7 +115,7 @@ __device__ inline EllipKE<T> ellip_agm(T m) {
   T a = 1, b = sqrt_t<T>(T(1) - m);
   T sum = T(0.5) * m;  // 2^(n-1) c_n², n = 0
   T pw = T(0.5);
-  for (int it = 0; it < 40; ++it) {
+  for (int it = 0; it < (m > T(0.9) ? 0 : 40); ++it) {
     const T c = T(0.5) * (a - b);
     const T an = T(0.5) * (a + b);
     b = sqrt_t<T>(a * b);
@@ -92,8 +124,12 @@ __device__ inline EllipKE<T> ellip_agm(T m) {
     sum += pw * c * c;
     if (fabs(c) <= tol * a) break;
   }
-  r.K = T(CUDART_PIO2) / a;
-  r.E = r.K * (T(1) - sum);
+  if (m > T(0.9)) {
+    ellip_comp_series<T, sizeof(T) == 8 ? 17 : 8>(T(1) - m, r.K, r.E);
+  } else {
+    r.K = T(CUDART_PIO2) / a;
+    r.E = r.K * (T(1) - sum);
+  }
   r.Kp = r.Ep = r.Kpp = r.Epp = 0;
   if (ORDER >= 1) {
     const T mc = T(1) - m;
@@ -137,36 +173,22 @@ __device__ inline EllipKE<T> ellip_eval(T m) {
     r.Epp = T(0);
     return r;
   }
-  const T small = sizeof(T) == 8 ? T(0.1) : T(0.3);
-  if (ORDER >= 1 && fabs(m) < small) return ellip_series<T, ORDER, sizeof(T) == 8 ? 20 : 16>(m);
+  // Below `small` the closed-form derivatives cancel by a factor ~1/m; the
+  // Maclaurin series is used instead (FP32 needs the wider band).
+  const T small = sizeof(T) == 8 ? T(0.1) : T(0.5);
+  if (ORDER >= 1 && fabs(m) < small) return ellip_series<T, ORDER, sizeof(T) == 8 ? 20 : 26>(m);
   return ellip_agm<T, ORDER>(m);
-}
-
-// Mixed: float AGM except near m = 1, where E = K(1 - Σ) cancels by a factor
-// ~K and the FP64 sweep is used.
-template <int ORDER>
-__device__ inline EllipKE<float> ellip_eval_m(float m) {
-  if (m > 0.9f && m < 1.0f) {
-    const EllipKE<double> d = ellip_eval<double, ORDER>((double)m);
-    EllipKE<float> r;
-    r.K = (float)d.K;
-    r.E = (float)d.E;
-    r.Kp = (float)d.Kp;
-    r.Ep = (float)d.Ep;
-    r.Kpp = (float)d.Kpp;
-    r.Epp = (float)d.Epp;
-    return r;
-  }
-  return ellip_eval<float, ORDER>(m);
 }
 
 template <int ORDER>
 __device__ __forceinline__ EllipKE<double> ellip_t(double m) {
   return ellip_eval<double, ORDER>(m);
 }
+// Mixed kernels: the same algorithms entirely in FP32 (the complementary
+// series removes the only cancellation that needed FP64).
 template <int ORDER>
 __device__ __forceinline__ EllipKE<float> ellip_t(float m) {
-  return ellip_eval_m<ORDER>(m);
+  return ellip_eval<float, ORDER>(m);
 }
 
 }  // namespace tsb

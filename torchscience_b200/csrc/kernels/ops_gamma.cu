@@ -3,11 +3,12 @@
 // their *_backward / *_backward_backward headers (same formulas:
 // d lnΓ = ψ, dΓ = Γψ, d²Γ = Γ(ψ² + ψ'), dψ = ψ', dψ' = ψ'').
 //
-// FP64 kernels (double data) evaluate everything in double with one region.
-// Mixed kernels (float/half/bf16 data) classify each element into region 0
-// (FP32 evaluation) or region 1 (FP64 evaluation of the same formula, for
-// arguments the FP32 path would not hold to 1e-6); the map kernel's
-// compaction keeps the two paths in separate warps.
+// FP64 kernels (double data) evaluate everything in double.  Mixed kernels
+// (float/half/bf16 data) evaluate in FP32 and send the rare arguments the
+// FP32 path would not hold to 1e-6 (x <= 0: reflection and the negative
+// zeros) through the FP64 evaluator of the same formula.  The rescue is rare
+// enough that a divergent branch costs less than staging the tile through
+// shared memory for compaction.
 #include <type_traits>
 
 #include "dispatch.cuh"
@@ -15,48 +16,51 @@
 
 namespace tsb {
 
+// Per-function traits: f0 = value; s1(s, z) = s·f'(z); s2(s, z) = s·f''(z)
+// (the scale s is applied where it keeps FP32 intermediates in range);
+// rescue(z): FP32 argument that takes the FP64 path in the mixed kernels.
 struct LogGammaFn {
   template <class T> __device__ static T f0(T z) { return lgamma_t(z); }
-  template <class T> __device__ static T f1(T z) { return digamma_t(z); }
-  template <class T> __device__ static T f2(T z) { return trigamma_t(z); }
-  // lnΓ cancels near its zeros at 1 and 2; x <= 0 uses reflection.
-  __device__ static bool rescue(float z) { return !(z > 0.0f) || (z > 0.5f && z < 3.0f); }
+  template <class T> __device__ static T s1(T s, T z) { return s * digamma_t(z); }
+  template <class T> __device__ static T s2(T s, T z) { return s * trigamma_t(z); }
+  __device__ static bool rescue(float z) { return !(z > 0.0f); }
 };
 struct GammaFn {
   template <class T> __device__ static T f0(T z) { return gamma_t(z); }
-  template <class T> __device__ static T f1(T z) { return gamma_t(z) * digamma_t(z); }
-  template <class T> __device__ static T f2(T z) {
+  // (s·ψ)·Γ: Γψ alone overflows float for z ~ 35 even when s·Γψ does not.
+  template <class T> __device__ static T s1(T s, T z) { return (s * digamma_t(z)) * gamma_t(z); }
+  template <class T> __device__ static T s2(T s, T z) {
     const T p = digamma_t(z);
-    return gamma_t(z) * (p * p + trigamma_t(z));
+    return (s * (p * p + trigamma_t(z))) * gamma_t(z);
   }
-  // Γψ and Γ(ψ²+ψ') overflow float before the upstream gradient scales them.
-  __device__ static bool rescue(float z) { return !(z > 0.0f) || z > 30.0f; }
+  __device__ static bool rescue(float z) { return !(z > 0.0f); }
 };
 struct DigammaFn {
   template <class T> __device__ static T f0(T z) { return digamma_t(z); }
-  template <class T> __device__ static T f1(T z) { return trigamma_t(z); }
-  template <class T> __device__ static T f2(T z) { return tetragamma_t(z); }
+  template <class T> __device__ static T s1(T s, T z) { return s * trigamma_t(z); }
+  template <class T> __device__ static T s2(T s, T z) { return s * tetragamma_t(z); }
   __device__ static bool rescue(float z) { return !(z > 1e-3f); }
 };
 struct TrigammaFn {
   template <class T> __device__ static T f0(T z) { return trigamma_t(z); }
-  template <class T> __device__ static T f1(T z) { return tetragamma_t(z); }
-  template <class T> __device__ static T f2(T z) { return pentagamma_t(z); }
+  template <class T> __device__ static T s1(T s, T z) { return s * tetragamma_t(z); }
+  template <class T> __device__ static T s2(T s, T z) { return s * pentagamma_t(z); }
   __device__ static bool rescue(float z) { return !(z > 1e-2f); }
 };
 
 template <typename T>
-constexpr int kMixedRegions = std::is_same<T, float>::value ? 2 : 1;
+__device__ __forceinline__ bool needs_fp64(bool rescue) {
+  return std::is_same<T, float>::value && rescue;
+}
 
 // Forward: out = f(z).
 template <class F, typename T_>
 struct UnaryFwd {
   using T = T_;
-  static constexpr int NIN = 1, NOUT = 1, R = kMixedRegions<T_>;
+  static constexpr int NIN = 1, NOUT = 1, R = 1;
   static constexpr bool REDUCE = false;
-  __device__ static int classify(const T* in) { return F::rescue((float)in[0]) ? 1 : 0; }
-  __device__ static void eval(int r, const T* in, T* out, uint32_t) {
-    if (R == 2 && r == 1) out[0] = (T)F::f0((double)in[0]);
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    if (needs_fp64<T>(F::rescue((float)in[0]))) out[0] = (T)F::f0((double)in[0]);
     else out[0] = F::f0(in[0]);
   }
 };
@@ -65,12 +69,11 @@ struct UnaryFwd {
 template <class F, typename T_>
 struct UnaryBwd {
   using T = T_;
-  static constexpr int NIN = 2, NOUT = 1, R = kMixedRegions<T_>;
+  static constexpr int NIN = 2, NOUT = 1, R = 1;
   static constexpr bool REDUCE = false;
-  __device__ static int classify(const T* in) { return F::rescue((float)in[1]) ? 1 : 0; }
-  __device__ static void eval(int r, const T* in, T* out, uint32_t) {
-    if (R == 2 && r == 1) out[0] = (T)((double)in[0] * F::f1((double)in[1]));
-    else out[0] = in[0] * F::f1(in[1]);
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    if (needs_fp64<T>(F::rescue((float)in[1]))) out[0] = (T)F::s1((double)in[0], (double)in[1]);
+    else out[0] = F::s1(in[0], in[1]);
   }
 };
 
@@ -78,17 +81,16 @@ struct UnaryBwd {
 template <class F, typename T_>
 struct UnaryBwdBwd {
   using T = T_;
-  static constexpr int NIN = 3, NOUT = 2, R = kMixedRegions<T_>;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
   static constexpr bool REDUCE = true;
-  __device__ static int classify(const T* in) { return F::rescue((float)in[2]) ? 1 : 0; }
-  __device__ static void eval(int r, const T* in, T* out, uint32_t mask) {
-    if (R == 2 && r == 1) {
+  __device__ static void eval(int, const T* in, T* out, uint32_t mask) {
+    if (needs_fp64<T>(F::rescue((float)in[2]))) {
       const double gg = in[0], g = in[1], z = in[2];
-      out[0] = (mask & 1u) ? (T)(gg * F::f1(z)) : T(0);
-      out[1] = (mask & 2u) ? (T)(gg * g * F::f2(z)) : T(0);
+      out[0] = (mask & 1u) ? (T)F::s1(gg, z) : T(0);
+      out[1] = (mask & 2u) ? (T)F::s2(gg * g, z) : T(0);
     } else {
-      out[0] = (mask & 1u) ? in[0] * F::f1(in[2]) : T(0);
-      out[1] = (mask & 2u) ? in[0] * in[1] * F::f2(in[2]) : T(0);
+      out[0] = (mask & 1u) ? F::s1(in[0], in[2]) : T(0);
+      out[1] = (mask & 2u) ? F::s2(in[0] * in[1], in[2]) : T(0);
     }
   }
 };
