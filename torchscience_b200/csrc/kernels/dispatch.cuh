@@ -148,13 +148,13 @@ inline int64_t reduce_ws_bytes(const Canon& c, int n_in, const tsb_tensor* out, 
 }
 
 template <class K>
-inline int occupancy_for(K kernel, size_t smem, int dev) {
+inline int occupancy_for(K kernel, int block, size_t smem, int dev) {
   static int cache[64];
   int* slot = dev >= 0 && dev < 64 ? &cache[dev] : nullptr;
   if (slot && *slot > 0) return *slot;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kBlock, smem) != cudaSuccess || blocks < 1) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, block, smem) != cudaSuccess || blocks < 1) {
     cudaGetLastError();
     blocks = 1;
   }
@@ -170,22 +170,26 @@ inline int32_t check_launch(const char* what) {
 
 template <class Fn, typename TS>
 int32_t launch_map(const MapParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t stream, int dev, const DeviceInfo* info) {
-  constexpr size_t smem = Fn::R > 1 ? TileShape<Fn>::SMEM : 0;
-  const int occ = occupancy_for(map_kernel<Fn, TS>, smem, dev);
-  const int64_t ntiles = (p.numel + TileShape<Fn>::TILE - 1) / TileShape<Fn>::TILE;
-  const int64_t grid = std::min<int64_t>(ntiles, (int64_t)info->sm_count * occ);
-  map_kernel<Fn, TS><<<(unsigned)grid, kBlock, smem, stream>>>(p);
+  constexpr size_t smem = WarpStage<Fn>::SMEM;
+  constexpr int block = WarpStage<Fn>::BLOCK;
+  const int occ = occupancy_for(map_kernel<Fn, TS>, block, smem, dev);
+  const int64_t nchunks = (p.numel + kChunk - 1) / kChunk;
+  const int64_t ctas = (nchunks + WarpStage<Fn>::WARPS - 1) / WarpStage<Fn>::WARPS;
+  const int64_t grid = std::min<int64_t>(ctas, (int64_t)info->sm_count * occ);
+  map_kernel<Fn, TS><<<(unsigned)grid, block, smem, stream>>>(p);
   return check_launch("map kernel launch");
 }
 
 template <class Fn, typename TS>
 int32_t launch_reduce(const Reduce2DParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t stream, int dev,
                       const DeviceInfo* info) {
-  constexpr size_t smem = TileShape<Fn>::SMEM;
-  const int occ = occupancy_for(reduce2d_kernel<Fn, TS>, smem, dev);
+  constexpr size_t smem = WarpStage<Fn>::SMEM;
+  constexpr int block = WarpStage<Fn>::BLOCK;
+  const int occ = occupancy_for(reduce2d_kernel<Fn, TS>, block, smem, dev);
   const int64_t ntiles = p.n_row_tiles * p.n_col_tiles;
-  const int64_t grid = std::min<int64_t>(ntiles, (int64_t)info->sm_count * occ);
-  reduce2d_kernel<Fn, TS><<<(unsigned)grid, kBlock, smem, stream>>>(p);
+  const int64_t ctas = (ntiles + WarpStage<Fn>::WARPS - 1) / WarpStage<Fn>::WARPS;
+  const int64_t grid = std::min<int64_t>(ctas, (int64_t)info->sm_count * occ);
+  reduce2d_kernel<Fn, TS><<<(unsigned)grid, block, smem, stream>>>(p);
   int32_t st = check_launch("reduce kernel launch");
   if (st) return st;
   for (int o = 0; o < Fn::NOUT; ++o) {

@@ -1,4 +1,5 @@
-// lnΓ, Γ, ψ, ψ' — forward, backward and double-backward entry points.
+// lnΓ, Γ, ψ, ψ' — functors of the forward, backward and double-backward
+// entry points.
 // Reference scalar kernels: log_gamma.h, gamma.h, digamma.h, trigamma.h and
 // their *_backward / *_backward_backward headers (same formulas:
 // d lnΓ = ψ, dΓ = Γψ, d²Γ = Γ(ψ² + ψ'), dψ = ψ', dψ' = ψ'').
@@ -9,6 +10,8 @@
 // zeros) through the FP64 evaluator of the same formula.  The rescue is rare
 // enough that a divergent branch costs less than staging the tile through
 // shared memory for compaction.
+#pragma once
+
 #include <type_traits>
 
 #include "dispatch.cuh"
@@ -106,16 +109,3 @@ TSB_UNARY_ALIASES(Digamma, DigammaFn)
 TSB_UNARY_ALIASES(Trigamma, TrigammaFn)
 
 }  // namespace tsb
-
-TSB_DEFINE_OP(tsb_log_gamma, tsb::LogGammaFwd)
-TSB_DEFINE_OP(tsb_log_gamma_backward, tsb::LogGammaBwd)
-TSB_DEFINE_OP(tsb_log_gamma_backward_backward, tsb::LogGammaBwdBwd)
-TSB_DEFINE_OP(tsb_gamma, tsb::GammaFwd)
-TSB_DEFINE_OP(tsb_gamma_backward, tsb::GammaBwd)
-TSB_DEFINE_OP(tsb_gamma_backward_backward, tsb::GammaBwdBwd)
-TSB_DEFINE_OP(tsb_digamma, tsb::DigammaFwd)
-TSB_DEFINE_OP(tsb_digamma_backward, tsb::DigammaBwd)
-TSB_DEFINE_OP(tsb_digamma_backward_backward, tsb::DigammaBwdBwd)
-TSB_DEFINE_OP(tsb_trigamma, tsb::TrigammaFwd)
-TSB_DEFINE_OP(tsb_trigamma_backward, tsb::TrigammaBwd)
-TSB_DEFINE_OP(tsb_trigamma_backward_backward, tsb::TrigammaBwdBwd)

@@ -214,18 +214,29 @@ struct IgammaOut {
   double paa, pax, pxx;
 };
 
-// Region ids shared by the classifier and the evaluators.
+// Region ids shared by the classifier and the evaluators.  Besides the
+// method (series / continued fraction / small-a / saturated), the series and
+// continued-fraction regions are split by the ratio that sets their
+// iteration count, so the lanes of a warp run loops of similar length.
 enum IgammaRegion : int {
-  kIgSpecial = 0,  // NaN / domain / x == 0 / x == inf / saturated (P = 0 or 1)
-  kIgSeriesLight = 1,
-  kIgSeriesHeavy = 2,
-  kIgCfLight = 3,
-  kIgCfHeavy = 4,
-  kIgSmallA = 5,  // a < 1, x < a + 1: series for P, dedicated formula for Q
-  kIgSat0 = 6,    // P and every derivative underflow to 0 (Q = 1)
-  kIgSat1 = 7,    // Q and every derivative underflow to 0 (P = 1)
-  kIgRegions = 8
+  kIgSpecial = 0,  // NaN / domain / x == 0 / x == inf
+  kIgS0 = 1,       // series, x/(a+1) < 0.1
+  kIgS1 = 2,       // series, x/(a+1) < 0.35
+  kIgS2 = 3,       // series, x/(a+1) < 0.7
+  kIgS3 = 4,       // series, x/(a+1) < 1
+  kIgC0 = 5,       // continued fraction, x/(a+1) > 3
+  kIgC1 = 6,       // continued fraction, x/(a+1) > 1.5
+  kIgC2 = 7,       // continued fraction, x/(a+1) <= 1.5
+  kIgSmallA = 8,   // a < 1, x < a + 1: series for P, dedicated formula for Q
+  kIgSat0 = 9,     // P and every derivative underflow to 0 (Q = 1)
+  kIgSat1 = 10,    // Q and every derivative underflow to 0 (P = 1)
+  kIgRegions = 11
 };
+
+// Regions whose loops are short enough for FP32 accumulation (mixed kernels).
+__device__ __forceinline__ bool igamma_fp32_ok(int region) {
+  return region == kIgS0 || region == kIgS1 || region == kIgC0;
+}
 
 // Region of (a, x) from cheap float arithmetic.
 __device__ __forceinline__ int igamma_classify(double ad, double xd) {
@@ -238,15 +249,16 @@ __device__ __forceinline__ int igamma_classify(double ad, double xd) {
   // The float estimate is good to far better than the 15-unit margin to the
   // double underflow threshold e^-745.
   const float lratio = fmaxf(0.0f, __logf(a / x));
+  const float lam = x / (a + 1.0f);
   if (x < a + 1.0f) {
     // P <= D·(a+1)/(a+1-x) ~ D·a.
     if (lnd + __logf(a + 1.0f) + lratio < -760.0f) return kIgSat0;
     if (a < 1.0f) return kIgSmallA;
-    return (x < 0.5f * (a + 1.0f)) ? kIgSeriesLight : kIgSeriesHeavy;
+    return lam < 0.1f ? kIgS0 : lam < 0.35f ? kIgS1 : lam < 0.7f ? kIgS2 : kIgS3;
   }
   // Q = a D F with F <= 1/(x+1-a) <= 1.
   if (lnd + __logf(a) + lratio < -760.0f) return kIgSat1;
-  return (x > 2.0f * (a + 1.0f) + 10.0f) ? kIgCfLight : kIgCfHeavy;
+  return lam > 3.0f ? kIgC0 : lam > 1.5f ? kIgC1 : kIgC2;
 }
 
 // Q(a, x) for a < 1, x < a + 1 without the 1 - P cancellation (P -> 1 as
@@ -358,9 +370,9 @@ template <int ORDER, bool WANT_Q = false>
 __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf) {
   if (region == kIgSmallA) {
     if (WANT_Q) return igamma_eval_d<ORDER, true>((double)af, (double)xf);
-    region = kIgSeriesLight;
+    region = kIgS1;
   }
-  if (region != kIgSeriesLight && region != kIgCfLight) return igamma_eval_d<ORDER>((double)af, (double)xf);
+  if (!igamma_fp32_ok(region)) return igamma_eval_d<ORDER>((double)af, (double)xf);
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
   const double a = af, x = xf;
@@ -370,7 +382,7 @@ __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf) {
   if (ORDER >= 1) psi_a = digamma_d(a);
   if (ORDER >= 2) psi1_a = trigamma_d(a);
   const double lx = log(x);
-  if (region == kIgSeriesLight) {
+  if (region != kIgC0) {
     float Sf, S1f = 0.0f, S2f = 0.0f;
     igamma_series<float, ORDER>(af, xf, Sf, S1f, S2f);
     const double S = Sf, S1 = S1f, S2 = S2f;

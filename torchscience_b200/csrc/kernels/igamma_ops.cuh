@@ -1,8 +1,10 @@
-// Regularized incomplete gamma P(a,x) and Q(a,x) = 1 - P: forward, backward
-// (grad_a, grad_x) and double-backward entry points.  Output conventions
+// Regularized incomplete gamma P(a,x) and Q(a,x) = 1 - P: functors of the
+// forward, backward (grad_a, grad_x) and double-backward entry points.  Output conventions
 // follow regularized_gamma_p_backward.h:27-33 and
 // regularized_gamma_p_backward_backward.h:12-41 (Q negates every derivative,
 // regularized_gamma_q_backward_backward.h:16-21).
+#pragma once
+
 #include "dispatch.cuh"
 #include "igamma_math.cuh"
 
@@ -71,10 +73,3 @@ template <typename T> using GammaQBwd = IgammaBwd<T, true>;
 template <typename T> using GammaQBwdBwd = IgammaBwdBwd<T, true>;
 
 }  // namespace tsb
-
-TSB_DEFINE_OP(tsb_regularized_gamma_p, tsb::GammaPFwd)
-TSB_DEFINE_OP(tsb_regularized_gamma_p_backward, tsb::GammaPBwd)
-TSB_DEFINE_OP(tsb_regularized_gamma_p_backward_backward, tsb::GammaPBwdBwd)
-TSB_DEFINE_OP(tsb_regularized_gamma_q, tsb::GammaQFwd)
-TSB_DEFINE_OP(tsb_regularized_gamma_q_backward, tsb::GammaQBwd)
-TSB_DEFINE_OP(tsb_regularized_gamma_q_backward_backward, tsb::GammaQBwdBwd)

@@ -7,19 +7,20 @@
 //   __device__ static int  classify(const T* in);              (R > 1 only)
 //   __device__ static void eval(int region, const T* in, T* out, uint32_t mask);
 //
-// When R > 1 each CTA works on a tile of TILE elements in four phases:
-//   1. coalesced load of the tile's inputs (strided/broadcast gather through
-//      the operand strides, or a dense fast path), region id per element;
-//   2. compaction: per-warp __match_any_sync groups lanes with equal region,
-//      one shared-memory atomic per group reserves slots, so the tile's local
-//      indices end up bucketed by region in shared memory;
-//   3. evaluation: consecutive threads take consecutive slots, so every warp
-//      runs a single region's code path except at bucket boundaries;
-//   4. results go back through shared memory and leave as coalesced stores.
-// R == 1 functors skip the shared-memory staging.
+// When R > 1 each warp works on its own chunk of 256 elements (no CTA-wide
+// barriers, so warps never wait for one another):
+//   1. coalesced load of the chunk's inputs (strided/broadcast gather through
+//      the operand strides, or a dense fast path) into a per-warp shared
+//      memory slice, and a region id per element;
+//   2. a ballot/popc prefix pass sorts the chunk's local indices by region
+//      (deterministic order);
+//   3. the warp evaluates the sorted list 32 at a time, so each round runs
+//      one region's code path except at region boundaries;
+//   4. results leave through the slice as coalesced stores.
+// R == 1 functors skip the staging and evaluate straight from registers.
 //
 // The 2-D variant (reduce2d_kernel) tiles an R x C iteration space in
-// TR x 32 blocks and sums outputs whose stride is zero along a dimension:
+// 8 x 32 blocks and sums outputs whose stride is zero along a dimension:
 // per-tile row/column partial sums in double land in a workspace and a
 // second kernel adds the partials in tile order, so results are
 // deterministic.  This is how backward kernels hand back gradients already
@@ -36,7 +37,7 @@
 namespace tsb {
 
 constexpr int kMaxDims = TSB_MAX_DIMS;
-constexpr int kBlock = 256;
+constexpr int kBlock = 256;  // block size of the finalize kernels
 
 struct Operand {
   char* ptr;
@@ -168,90 +169,101 @@ __device__ __forceinline__ void store_element(const MapParams<Fn::NIN, Fn::NOUT>
   }
 }
 
+// ------------------------------------------------------------ warp chunks
+// Every warp works on its own chunk of kChunk = 8 x 32 elements, independent
+// of the other warps of its CTA (no block-wide barriers: a warp whose chunk
+// holds long continued fractions does not hold up its neighbours).
+constexpr int kEPT = 8;            // elements per lane per chunk
+constexpr int kChunk = 32 * kEPT;  // 256
+constexpr int kTC = 32;            // 2-D tile columns (one per lane)
+constexpr int kTR = kEPT;          // 2-D tile rows
+
 template <class Fn>
-struct TileShape {
+struct WarpStage {
+  using T = typename Fn::T;
   static constexpr int NBUF = Fn::NIN > Fn::NOUT ? Fn::NIN : Fn::NOUT;
-  static constexpr int EPT = 4;
-  static constexpr int TILE = kBlock * EPT;  // 1024 elements
-  // Dynamic shared memory: staging buffer + region list + region ids.
-  static constexpr size_t SMEM = (size_t)NBUF * TILE * sizeof(typename Fn::T) + TILE * sizeof(uint16_t) + TILE;
+  // Per-warp shared memory: operand staging + region-sorted list + regions.
+  static constexpr size_t PER_WARP = (size_t)NBUF * kChunk * sizeof(T) + 2 * kChunk;
+  // Warps per CTA: at most 8, fewer when a warp's slice is large.
+  static constexpr int WARPS = PER_WARP * 8 <= 64 * 1024 ? 8 : PER_WARP * 4 <= 64 * 1024 ? 4 : 2;
+  static constexpr int BLOCK = 32 * WARPS;
+  static constexpr size_t SMEM = Fn::R > 1 ? PER_WARP * WARPS : 0;
 };
 
-template <class Fn>
-__device__ __forceinline__ void carve_smem(unsigned char* base, typename Fn::T*& buf, uint16_t*& list,
-                                           uint8_t*& reg) {
-  using T = typename Fn::T;
-  buf = reinterpret_cast<T*>(base);
-  list = reinterpret_cast<uint16_t*>(buf + TileShape<Fn>::NBUF * TileShape<Fn>::TILE);
-  reg = reinterpret_cast<uint8_t*>(list + TileShape<Fn>::TILE);
+// Sorts the chunk's local indices by region with ballot prefix counts
+// (deterministic order); returns the number of valid elements.  reg[k] is
+// the region of local index k*32 + lane, or R for an invalid slot.
+template <int R>
+__device__ __forceinline__ int warp_sort_by_region(const int (&reg)[kEPT], uint8_t* list, uint8_t* regs) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  int count = 0;
+#pragma unroll
+  for (int k = 0; k < kEPT; ++k) regs[k * 32 + lane] = static_cast<uint8_t>(reg[k]);
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+#pragma unroll
+    for (int k = 0; k < kEPT; ++k) {
+      const unsigned m = __ballot_sync(0xffffffffu, reg[k] == r);
+      if (reg[k] == r) list[count + __popc(m & lt)] = static_cast<uint8_t>(k * 32 + lane);
+      count += __popc(m);
+    }
+  }
+  __syncwarp();
+  return count;
 }
 
-// Bucket the tile's local indices by region.  `reg[k]` is the region of the
-// element at local index k*kBlock + tid, or R (not valid).  On return
-// s_list[0..count) holds local indices grouped by region, and s_reg[li] the
-// region of local index li.
-template <int R, int EPT>
-__device__ __forceinline__ int compact_by_region(const int (&reg)[EPT], uint16_t* s_list,
-                                                 uint8_t* s_reg, int* s_cnt) {
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  if (tid < R) s_cnt[tid] = 0;
-  __syncthreads();
+// Evaluates the sorted chunk in place: inputs are read from, and outputs
+// written to, the staging slots of each local index.
+template <class Fn>
+__device__ __forceinline__ void warp_eval_sorted(int count, typename Fn::T* buf, const uint8_t* list,
+                                                 const uint8_t* regs, uint32_t mask) {
+  using T = typename Fn::T;
+  const int lane = threadIdx.x & 31;
+  for (int j = lane; j < count; j += 32) {
+    const int li = list[j];
+    T v[Fn::NIN], o[Fn::NOUT];
 #pragma unroll
-  for (int k = 0; k < EPT; ++k) {
-    const unsigned grp = __match_any_sync(0xffffffffu, reg[k]);
-    const int leader = __ffs(grp) - 1;
-    if (lane == leader && reg[k] < R) atomicAdd(&s_cnt[reg[k]], __popc(grp));
-    s_reg[k * kBlock + tid] = static_cast<uint8_t>(reg[k]);
-  }
-  __syncthreads();
-  // Exclusive scan over the R region counters (R is small).
-  __shared__ int s_base[R + 1];
-  if (tid == 0) {
-    int acc = 0;
+    for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * kChunk + li];
+    Fn::eval(regs[li], v, o, mask);
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      s_base[r] = acc;
-      acc += s_cnt[r];
-    }
-    s_base[R] = acc;
+    for (int q = 0; q < Fn::NOUT; ++q) buf[q * kChunk + li] = o[q];
   }
-  __syncthreads();
-  if (tid < R) s_cnt[tid] = s_base[tid];  // reuse as running cursor
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < EPT; ++k) {
-    const unsigned grp = __match_any_sync(0xffffffffu, reg[k]);
-    const int leader = __ffs(grp) - 1;
-    int pos = 0;
-    if (lane == leader && reg[k] < R) pos = atomicAdd(&s_cnt[reg[k]], __popc(grp));
-    pos = __shfl_sync(0xffffffffu, pos, leader);
-    if (reg[k] < R) s_list[pos + __popc(grp & lt_mask)] = static_cast<uint16_t>(k * kBlock + tid);
-  }
-  __syncthreads();
-  return s_base[R];
+  __syncwarp();
+}
+
+template <class Fn>
+__device__ __forceinline__ void warp_slice(unsigned char* base, typename Fn::T*& buf, uint8_t*& list,
+                                           uint8_t*& regs) {
+  using T = typename Fn::T;
+  const int warp = threadIdx.x >> 5;
+  unsigned char* w = base + warp * WarpStage<Fn>::PER_WARP;
+  buf = reinterpret_cast<T*>(w);
+  list = w + (size_t)WarpStage<Fn>::NBUF * kChunk * sizeof(T);
+  regs = list + kChunk;
 }
 
 template <class Fn, typename TS>
-__global__ void __launch_bounds__(kBlock) map_kernel(const MapParams<Fn::NIN, Fn::NOUT> p) {
+__global__ void __launch_bounds__(256) map_kernel(const MapParams<Fn::NIN, Fn::NOUT> p) {
   using T = typename Fn::T;
   constexpr int NIN = Fn::NIN, NOUT = Fn::NOUT, R = Fn::R;
-  constexpr int EPT = TileShape<Fn>::EPT, TILE = TileShape<Fn>::TILE, NBUF = TileShape<Fn>::NBUF;
-  const int64_t ntiles = (p.numel + TILE - 1) / TILE;
-  const int tid = threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t nchunks = (p.numel + kChunk - 1) / kChunk;
+  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
 
   if constexpr (R == 1) {
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      T v[EPT][NIN];
+    for (int64_t c = wid; c < nchunks; c += nw) {
+      const int64_t base = c * kChunk;
+      T v[kEPT][NIN];
 #pragma unroll
-      for (int k = 0; k < EPT; ++k) {
-        const int64_t i = t * TILE + k * kBlock + tid;
+      for (int k = 0; k < kEPT; ++k) {
+        const int64_t i = base + k * 32 + lane;
         if (i < p.numel) load_element<Fn, TS>(p, i, v[k]);
       }
 #pragma unroll
-      for (int k = 0; k < EPT; ++k) {
-        const int64_t i = t * TILE + k * kBlock + tid;
+      for (int k = 0; k < kEPT; ++k) {
+        const int64_t i = base + k * 32 + lane;
         if (i < p.numel) {
           T o[NOUT];
           Fn::eval(0, v[k], o, p.out_mask);
@@ -261,17 +273,15 @@ __global__ void __launch_bounds__(kBlock) map_kernel(const MapParams<Fn::NIN, Fn
     }
   } else {
     extern __shared__ __align__(16) unsigned char s_dyn[];
-    T* s_buf;
-    uint16_t* s_list;
-    uint8_t* s_reg;
-    carve_smem<Fn>(s_dyn, s_buf, s_list, s_reg);
-    __shared__ int s_cnt[R];
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      const int64_t base = t * TILE;
-      int reg[EPT];
+    T* buf;
+    uint8_t *list, *regs;
+    warp_slice<Fn>(s_dyn, buf, list, regs);
+    for (int64_t c = wid; c < nchunks; c += nw) {
+      const int64_t base = c * kChunk;
+      int reg[kEPT];
 #pragma unroll
-      for (int k = 0; k < EPT; ++k) {
-        const int li = k * kBlock + tid;
+      for (int k = 0; k < kEPT; ++k) {
+        const int li = k * 32 + lane;
         const int64_t i = base + li;
         reg[k] = R;
         if (i < p.numel) {
@@ -279,174 +289,125 @@ __global__ void __launch_bounds__(kBlock) map_kernel(const MapParams<Fn::NIN, Fn
           load_element<Fn, TS>(p, i, v);
           reg[k] = Fn::classify(v);
 #pragma unroll
-          for (int q = 0; q < NIN; ++q) s_buf[q * TILE + li] = v[q];
+          for (int q = 0; q < NIN; ++q) buf[q * kChunk + li] = v[q];
         }
       }
-      const int count = compact_by_region<R, EPT>(reg, s_list, s_reg, s_cnt);
-      for (int j = tid; j < count; j += kBlock) {
-        const int li = s_list[j];
-        T v[NIN], o[NOUT];
+      __syncwarp();
+      const int count = warp_sort_by_region<R>(reg, list, regs);
+      warp_eval_sorted<Fn>(count, buf, list, regs, p.out_mask);
 #pragma unroll
-        for (int q = 0; q < NIN; ++q) v[q] = s_buf[q * TILE + li];
-        Fn::eval(s_reg[li], v, o, p.out_mask);
-#pragma unroll
-        for (int q = 0; q < NOUT; ++q) s_buf[q * TILE + li] = o[q];
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < EPT; ++k) {
-        const int li = k * kBlock + tid;
+      for (int k = 0; k < kEPT; ++k) {
+        const int li = k * 32 + lane;
         const int64_t i = base + li;
         if (i < p.numel) {
           T o[NOUT];
 #pragma unroll
-          for (int q = 0; q < NOUT; ++q) o[q] = s_buf[q * TILE + li];
+          for (int q = 0; q < NOUT; ++q) o[q] = buf[q * kChunk + li];
           store_element<Fn, TS>(p, i, o);
         }
       }
-      __syncthreads();
+      __syncwarp();
     }
   }
 }
 
 // ------------------------------------------------------------ 2-D reduction
-constexpr int kTC = 32;  // tile columns (one warp wide)
-constexpr int kTR = 1024 / kTC;  // tile rows (tiles hold 1024 elements)
-
-template <class Fn>
-struct Tile2D {
-  static constexpr int TILE = TileShape<Fn>::TILE;
-  static constexpr int TR = TILE / kTC;
-  static_assert(TR == kTR, "2-D tiles are 32 x 32");
-};
-
+// Tiles of kTR rows x 32 columns, one per warp chunk: lane = column, the
+// lane's kEPT elements are the tile's rows.  Row-reduced outputs take a
+// shuffle tree per row, column-reduced outputs a fixed-order sum over the
+// lane's rows; per-tile partials (double) go to the workspace.
 template <class Fn, typename TS>
-__global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<Fn::NIN, Fn::NOUT> p) {
+__global__ void __launch_bounds__(256) reduce2d_kernel(const Reduce2DParams<Fn::NIN, Fn::NOUT> p) {
   using T = typename Fn::T;
   constexpr int NIN = Fn::NIN, NOUT = Fn::NOUT, R = Fn::R;
-  constexpr int EPT = TileShape<Fn>::EPT, TILE = TileShape<Fn>::TILE, NBUF = TileShape<Fn>::NBUF;
-  constexpr int TR = Tile2D<Fn>::TR;
-  constexpr int RR = R > 1 ? R : 1;
-  extern __shared__ __align__(16) unsigned char s_dyn[];
-  T* s_buf;
-  uint16_t* s_list;
-  uint8_t* s_reg;
-  carve_smem<Fn>(s_dyn, s_buf, s_list, s_reg);
-  __shared__ int s_cnt[RR];
-  __shared__ double s_red[kBlock / 32][kTC];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int lane = threadIdx.x & 31;
   const int64_t ntiles = p.n_row_tiles * p.n_col_tiles;
+  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  T* buf = nullptr;
+  uint8_t *list = nullptr, *regs = nullptr;
+  if constexpr (R > 1) warp_slice<Fn>(s_dyn, buf, list, regs);
 
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (int64_t t = wid; t < ntiles; t += nw) {
     const int64_t rt = t / p.n_col_tiles, ct = t % p.n_col_tiles;
-    const int64_t r0 = rt * TR, c0 = ct * kTC;
-    int reg[EPT];
+    const int64_t r0 = rt * kTR, c = ct * kTC + lane;
+    const bool col_ok = c < p.cols;
+    T res[kEPT][NOUT];
+    bool ok[kEPT];
 #pragma unroll
-    for (int k = 0; k < EPT; ++k) {
-      const int li = k * kBlock + tid;
-      const int64_t r = r0 + li / kTC, c = c0 + li % kTC;
-      reg[k] = R;
-      if (r < p.rows && c < p.cols) {
-        T v[NIN];
+    for (int k = 0; k < kEPT; ++k) ok[k] = col_ok && (r0 + k) < p.rows;
+
+    if constexpr (R == 1) {
 #pragma unroll
-        for (int q = 0; q < NIN; ++q)
-          v[q] = load_as<TS, T>(p.in_ptr[q] + (r * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
-        if constexpr (R > 1) reg[k] = Fn::classify(v);
-        else reg[k] = 0;
+      for (int k = 0; k < kEPT; ++k) {
+        if (ok[k]) {
+          T v[NIN];
 #pragma unroll
-        for (int q = 0; q < NIN; ++q) s_buf[q * TILE + li] = v[q];
-      }
-    }
-    int count;
-    if constexpr (R > 1) {
-      count = compact_by_region<R, EPT>(reg, s_list, s_reg, s_cnt);
-    } else {
-      // No compaction: each thread evaluates its own elements in place.
-      count = -1;
-      __syncthreads();
-    }
-    if (count >= 0) {
-      for (int j = tid; j < count; j += kBlock) {
-        const int li = s_list[j];
-        T v[NIN], o[NOUT];
+          for (int q = 0; q < NIN; ++q)
+            v[q] = load_as<TS, T>(p.in_ptr[q] + ((r0 + k) * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
+          Fn::eval(0, v, res[k], p.out_mask);
+        } else {
 #pragma unroll
-        for (int q = 0; q < NIN; ++q) v[q] = s_buf[q * TILE + li];
-        Fn::eval(s_reg[li], v, o, p.out_mask);
-#pragma unroll
-        for (int q = 0; q < NOUT; ++q) s_buf[q * TILE + li] = o[q];
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < EPT; ++k) {
-        const int li = k * kBlock + tid;
-        if (reg[k] < R) {
-          const int64_t r = r0 + li / kTC, c = c0 + li % kTC;
-          if (r < p.rows && c < p.cols) {
-            T v[NIN], o[NOUT];
-#pragma unroll
-            for (int q = 0; q < NIN; ++q) v[q] = s_buf[q * TILE + li];
-            Fn::eval(0, v, o, p.out_mask);
-#pragma unroll
-            for (int q = 0; q < NOUT; ++q) s_buf[q * TILE + li] = o[q];
-          }
+          for (int q = 0; q < NOUT; ++q) res[k][q] = T(0);
         }
       }
+    } else {
+      int reg[kEPT];
+#pragma unroll
+      for (int k = 0; k < kEPT; ++k) {
+        const int li = k * 32 + lane;
+        reg[k] = R;
+        if (ok[k]) {
+          T v[NIN];
+#pragma unroll
+          for (int q = 0; q < NIN; ++q)
+            v[q] = load_as<TS, T>(p.in_ptr[q] + ((r0 + k) * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
+          reg[k] = Fn::classify(v);
+#pragma unroll
+          for (int q = 0; q < NIN; ++q) buf[q * kChunk + li] = v[q];
+        }
+      }
+      __syncwarp();
+      const int count = warp_sort_by_region<R>(reg, list, regs);
+      warp_eval_sorted<Fn>(count, buf, list, regs, p.out_mask);
+#pragma unroll
+      for (int k = 0; k < kEPT; ++k)
+#pragma unroll
+        for (int q = 0; q < NOUT; ++q) res[k][q] = ok[k] ? buf[q * kChunk + k * 32 + lane] : T(0);
+      __syncwarp();
     }
-    __syncthreads();
 
-    const int rows_here = (int)(p.rows - r0 < (int64_t)TR ? p.rows - r0 : (int64_t)TR);
-    const int cols_here = (int)(p.cols - c0 < (int64_t)kTC ? p.cols - c0 : (int64_t)kTC);
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
       if (!(p.out_mask & (1u << o))) continue;
       const int kind = p.out_kind[o];
       if (kind == kOutFull) {
 #pragma unroll
-        for (int k = 0; k < EPT; ++k) {
-          const int li = k * kBlock + tid;
-          const int lr = li / kTC, lc = li % kTC;
-          if (lr < rows_here && lc < cols_here)
-            store_as<TS>(p.out_ptr[o] + ((r0 + lr) * p.out_s0[o] + (c0 + lc) * p.out_s1[o]) * (int64_t)sizeof(TS),
-                         s_buf[o * TILE + li]);
-        }
-      } else if (kind == kOutRow || kind == kOutAll) {
-        // Row sums over this tile's columns: warp w takes rows w, w+8, ...
-        // lane = column; fixed shuffle tree => deterministic.
-        double tile_sum = 0.0;
-        for (int lr = warp; lr < TR; lr += kBlock / 32) {
-          double v = (lr < rows_here && lane < cols_here) ? (double)s_buf[o * TILE + lr * kTC + lane] : 0.0;
+        for (int k = 0; k < kEPT; ++k)
+          if (ok[k])
+            store_as<TS>(p.out_ptr[o] + ((r0 + k) * p.out_s0[o] + c * p.out_s1[o]) * (int64_t)sizeof(TS), res[k][o]);
+      } else if (kind == kOutRow) {
+#pragma unroll
+        for (int k = 0; k < kEPT; ++k) {
+          double v = (double)res[k][o];
 #pragma unroll
           for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-          if (kind == kOutRow) {
-            if (lane == 0 && lr < rows_here) p.ws[o][ct * p.rows + r0 + lr] = v;
-          } else {
-            tile_sum += v;
-          }
-        }
-        if (kind == kOutAll) {
-          if (lane == 0) s_red[warp][0] = tile_sum;
-          __syncthreads();
-          if (tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < kBlock / 32; ++w) s += s_red[w][0];
-            p.ws[o][t] = s;
-          }
+          if (lane == 0 && r0 + k < p.rows) p.ws[o][ct * p.rows + r0 + k] = v;
         }
       } else if (kind == kOutCol) {
-        // Column sums over this tile's rows: warp w sums rows w, w+8, ...
-        // per lane (= column), then warp partials are added in order.
         double v = 0.0;
-        for (int lr = warp; lr < rows_here; lr += kBlock / 32) v += (double)s_buf[o * TILE + lr * kTC + lane];
-        s_red[warp][lane] = v;
-        __syncthreads();
-        if (warp == 0) {
-          double s = 0.0;
 #pragma unroll
-          for (int w = 0; w < kBlock / 32; ++w) s += s_red[w][lane];
-          if (lane < cols_here) p.ws[o][rt * p.cols + c0 + lane] = s;
-        }
+        for (int k = 0; k < kEPT; ++k) v += (double)res[k][o];
+        if (col_ok) p.ws[o][rt * p.cols + c] = v;
+      } else if (kind == kOutAll) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < kEPT; ++k) v += (double)res[k][o];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) p.ws[o][t] = v;
       }
-      __syncthreads();
     }
   }
 }
