@@ -80,8 +80,8 @@ def test_workspace_query_for_the_broadcast_grid():
     ga = desc(shape, strides=[1, 0])
     gx = desc(shape, strides=[0, 1])
     n = L.tsb_workspace_bytes(arr(g, a, x), 3, arr(ga, gx), 2)
-    # row-reduced: 128 column tiles x 4096 rows; column-reduced: 512 row tiles (8 rows) x 4096 cols (doubles)
-    assert n == (128 + 512) * 4096 * 8
+    # row-reduced: 128 column tiles x 4096 rows; column-reduced: 128 row tiles (32 rows) x 4096 cols (doubles)
+    assert n == (128 + 128) * 4096 * 8
     # no reduced output -> 0
     assert L.tsb_workspace_bytes(arr(g, a, x), 3, arr(desc(shape), desc(shape)), 2) == 0
 

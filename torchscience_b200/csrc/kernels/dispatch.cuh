@@ -147,7 +147,10 @@ inline int64_t reduce_ws_bytes(const Canon& c, int n_in, const tsb_tensor* out, 
   return total;
 }
 
-template <class K>
+// Resident CTAs per SM for one kernel instantiation, cached per device.
+// `Tag` makes the cache (and the shared-memory opt-in) specific to the kernel:
+// kernels of different functors can share a signature type.
+template <class Tag, class K>
 inline int occupancy_for(K kernel, int block, size_t smem, int dev) {
   static int cache[64];
   int* slot = dev >= 0 && dev < 64 ? &cache[dev] : nullptr;
@@ -162,6 +165,11 @@ inline int occupancy_for(K kernel, int block, size_t smem, int dev) {
   return blocks;
 }
 
+template <class Fn, typename TS>
+struct MapTag {};
+template <class Fn, typename TS>
+struct ReduceTag {};
+
 inline int32_t check_launch(const char* what) {
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(TSB_ERR_LAUNCH, "%s: %s", what, cudaGetErrorString(e));
@@ -170,26 +178,23 @@ inline int32_t check_launch(const char* what) {
 
 template <class Fn, typename TS>
 int32_t launch_map(const MapParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t stream, int dev, const DeviceInfo* info) {
-  constexpr size_t smem = WarpStage<Fn>::SMEM;
-  constexpr int block = WarpStage<Fn>::BLOCK;
-  const int occ = occupancy_for(map_kernel<Fn, TS>, block, smem, dev);
-  const int64_t nchunks = (p.numel + kChunk - 1) / kChunk;
-  const int64_t ctas = (nchunks + WarpStage<Fn>::WARPS - 1) / WarpStage<Fn>::WARPS;
-  const int64_t grid = std::min<int64_t>(ctas, (int64_t)info->sm_count * occ);
-  map_kernel<Fn, TS><<<(unsigned)grid, block, smem, stream>>>(p);
+  using S = typename MapTile<Fn>::S;
+  constexpr size_t smem = Fn::R > 1 ? S::SMEM : 0;
+  const int occ = occupancy_for<MapTag<Fn, TS>>(map_kernel<Fn, TS>, kBlock, smem, dev);
+  const int64_t ntiles = (p.numel + S::TILE - 1) / S::TILE;
+  const int64_t grid = std::min<int64_t>(ntiles, (int64_t)info->sm_count * occ);
+  map_kernel<Fn, TS><<<(unsigned)grid, kBlock, smem, stream>>>(p);
   return check_launch("map kernel launch");
 }
 
 template <class Fn, typename TS>
 int32_t launch_reduce(const Reduce2DParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t stream, int dev,
                       const DeviceInfo* info) {
-  constexpr size_t smem = WarpStage<Fn>::SMEM;
-  constexpr int block = WarpStage<Fn>::BLOCK;
-  const int occ = occupancy_for(reduce2d_kernel<Fn, TS>, block, smem, dev);
+  constexpr size_t smem = ReduceStage<Fn>::SMEM;
+  const int occ = occupancy_for<ReduceTag<Fn, TS>>(reduce2d_kernel<Fn, TS>, kBlock, smem, dev);
   const int64_t ntiles = p.n_row_tiles * p.n_col_tiles;
-  const int64_t ctas = (ntiles + WarpStage<Fn>::WARPS - 1) / WarpStage<Fn>::WARPS;
-  const int64_t grid = std::min<int64_t>(ctas, (int64_t)info->sm_count * occ);
-  reduce2d_kernel<Fn, TS><<<(unsigned)grid, block, smem, stream>>>(p);
+  const int64_t grid = std::min<int64_t>(ntiles, (int64_t)info->sm_count * occ);
+  reduce2d_kernel<Fn, TS><<<(unsigned)grid, kBlock, smem, stream>>>(p);
   int32_t st = check_launch("reduce kernel launch");
   if (st) return st;
   for (int o = 0; o < Fn::NOUT; ++o) {

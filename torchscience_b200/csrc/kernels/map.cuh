@@ -7,20 +7,22 @@
 //   __device__ static int  classify(const T* in);              (R > 1 only)
 //   __device__ static void eval(int region, const T* in, T* out, uint32_t mask);
 //
-// When R > 1 each warp works on its own chunk of 256 elements (no CTA-wide
-// barriers, so warps never wait for one another):
-//   1. coalesced load of the chunk's inputs (strided/broadcast gather through
-//      the operand strides, or a dense fast path) into a per-warp shared
-//      memory slice, and a region id per element;
-//   2. a ballot/popc prefix pass sorts the chunk's local indices by region
-//      (deterministic order);
-//   3. the warp evaluates the sorted list 32 at a time, so each round runs
-//      one region's code path except at region boundaries;
-//   4. results leave through the slice as coalesced stores.
-// R == 1 functors skip the staging and evaluate straight from registers.
+// When R > 1 each CTA works on a tile of up to 2048 elements in four phases:
+//   1. coalesced load of the tile's inputs (strided/broadcast gather through
+//      the operand strides, or a dense fast path), region id per element;
+//   2. compaction: per-warp __match_any_sync groups lanes with equal region,
+//      one shared-memory atomic per group reserves slots, so the tile's local
+//      indices end up bucketed by region in shared memory;
+//   3. evaluation: consecutive threads take consecutive slots, so every warp
+//      runs a single region's code path except at bucket boundaries, and the
+//      32-slot groups go round-robin to the warps so their loads balance;
+//   4. results go back through shared memory and leave as coalesced stores.
+// R == 1 functors skip the shared-memory staging.  Regions are both the
+// evaluation method and, for iterative methods, a bucket of the expected
+// iteration count, so warps run loops of similar length.
 //
 // The 2-D variant (reduce2d_kernel) tiles an R x C iteration space in
-// 8 x 32 blocks and sums outputs whose stride is zero along a dimension:
+// 32 x 32 blocks and sums outputs whose stride is zero along a dimension:
 // per-tile row/column partial sums in double land in a workspace and a
 // second kernel adds the partials in tile order, so results are
 // deterministic.  This is how backward kernels hand back gradients already
@@ -37,7 +39,7 @@
 namespace tsb {
 
 constexpr int kMaxDims = TSB_MAX_DIMS;
-constexpr int kBlock = 256;  // block size of the finalize kernels
+constexpr int kBlock = 256;
 
 struct Operand {
   char* ptr;
@@ -169,101 +171,120 @@ __device__ __forceinline__ void store_element(const MapParams<Fn::NIN, Fn::NOUT>
   }
 }
 
-// ------------------------------------------------------------ warp chunks
-// Every warp works on its own chunk of kChunk = 8 x 32 elements, independent
-// of the other warps of its CTA (no block-wide barriers: a warp whose chunk
-// holds long continued fractions does not hold up its neighbours).
-constexpr int kEPT = 8;            // elements per lane per chunk
-constexpr int kChunk = 32 * kEPT;  // 256
-constexpr int kTC = 32;            // 2-D tile columns (one per lane)
-constexpr int kTR = kEPT;          // 2-D tile rows
+// ------------------------------------------------------------ CTA tiles
+// Map kernels stage tiles of up to 2048 elements (1024 when the operands
+// need more shared memory); the 2-D reduction uses 32 x 32 tiles.
+constexpr int kTC = 32;                 // 2-D tile columns (one per lane)
+constexpr int kTR = 32;                 // 2-D tile rows
+constexpr int kTile2D = kTC * kTR;      // 1024
 
-template <class Fn>
-struct WarpStage {
+template <class Fn, int TILE_>
+struct Stage {
   using T = typename Fn::T;
   static constexpr int NBUF = Fn::NIN > Fn::NOUT ? Fn::NIN : Fn::NOUT;
-  // Per-warp shared memory: operand staging + region-sorted list + regions.
-  static constexpr size_t PER_WARP = (size_t)NBUF * kChunk * sizeof(T) + 2 * kChunk;
-  // Warps per CTA: at most 8, fewer when a warp's slice is large.
-  static constexpr int WARPS = PER_WARP * 8 <= 64 * 1024 ? 8 : PER_WARP * 4 <= 64 * 1024 ? 4 : 2;
-  static constexpr int BLOCK = 32 * WARPS;
-  static constexpr size_t SMEM = Fn::R > 1 ? PER_WARP * WARPS : 0;
+  static constexpr int TILE = TILE_;
+  static constexpr int EPT = TILE / kBlock;
+  // operand staging + region-sorted list (uint16) + region ids (uint8)
+  static constexpr size_t SMEM = (size_t)NBUF * TILE * sizeof(T) + TILE * sizeof(uint16_t) + TILE;
 };
 
-// Sorts the chunk's local indices by region with ballot prefix counts
-// (deterministic order); returns the number of valid elements.  reg[k] is
-// the region of local index k*32 + lane, or R for an invalid slot.
-template <int R>
-__device__ __forceinline__ int warp_sort_by_region(const int (&reg)[kEPT], uint8_t* list, uint8_t* regs) {
-  const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1u;
-  int count = 0;
-#pragma unroll
-  for (int k = 0; k < kEPT; ++k) regs[k * 32 + lane] = static_cast<uint8_t>(reg[k]);
-#pragma unroll 1
-  for (int r = 0; r < R; ++r) {
-#pragma unroll
-    for (int k = 0; k < kEPT; ++k) {
-      const unsigned m = __ballot_sync(0xffffffffu, reg[k] == r);
-      if (reg[k] == r) list[count + __popc(m & lt)] = static_cast<uint8_t>(k * 32 + lane);
-      count += __popc(m);
-    }
-  }
-  __syncwarp();
-  return count;
+template <class Fn>
+struct MapTile {
+  static constexpr int BIG = Stage<Fn, 2048>::SMEM <= 64 * 1024 ? 2048 : 1024;
+  using S = Stage<Fn, (Fn::R > 1 ? BIG : 1024)>;
+};
+
+template <class S>
+__device__ __forceinline__ void carve(unsigned char* base, typename S::T*& buf, uint16_t*& list, uint8_t*& regs) {
+  using T = typename S::T;
+  buf = reinterpret_cast<T*>(base);
+  list = reinterpret_cast<uint16_t*>(buf + (size_t)S::NBUF * S::TILE);
+  regs = reinterpret_cast<uint8_t*>(list + S::TILE);
 }
 
-// Evaluates the sorted chunk in place: inputs are read from, and outputs
-// written to, the staging slots of each local index.
-template <class Fn>
-__device__ __forceinline__ void warp_eval_sorted(int count, typename Fn::T* buf, const uint8_t* list,
-                                                 const uint8_t* regs, uint32_t mask) {
+// Buckets the tile's local indices by region.  reg[k] is the region of
+// local index k*kBlock + tid, or R for an invalid slot.  On return
+// list[0..count) holds the valid local indices grouped by region and
+// regs[li] the region of li.  (Order inside a region depends on atomic
+// order; results do not, each element being evaluated independently.)
+template <int R, int EPT>
+__device__ __forceinline__ int cta_sort_by_region(const int (&reg)[EPT], uint16_t* list, uint8_t* regs, int* s_cnt,
+                                                  int* s_base) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  if (tid < R) s_cnt[tid] = 0;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < EPT; ++k) {
+    const unsigned grp = __match_any_sync(0xffffffffu, reg[k]);
+    if (lane == __ffs(grp) - 1 && reg[k] < R) atomicAdd(&s_cnt[reg[k]], __popc(grp));
+    regs[k * kBlock + tid] = static_cast<uint8_t>(reg[k]);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      s_base[r] = acc;
+      acc += s_cnt[r];
+    }
+    s_base[R] = acc;
+  }
+  __syncthreads();
+  if (tid < R) s_cnt[tid] = s_base[tid];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < EPT; ++k) {
+    const unsigned grp = __match_any_sync(0xffffffffu, reg[k]);
+    const int leader = __ffs(grp) - 1;
+    int pos = 0;
+    if (lane == leader && reg[k] < R) pos = atomicAdd(&s_cnt[reg[k]], __popc(grp));
+    pos = __shfl_sync(0xffffffffu, pos, leader);
+    if (reg[k] < R) list[pos + __popc(grp & lt)] = static_cast<uint16_t>(k * kBlock + tid);
+  }
+  __syncthreads();
+  return s_base[R];
+}
+
+// Evaluates the sorted tile in place.  Thread t takes sorted slots t,
+// t + kBlock, ...: warp w gets 32-slot groups w, w + 8, ..., a round-robin
+// spread of every region over the warps that keeps their loads balanced.
+template <class Fn, int TILE>
+__device__ __forceinline__ void cta_eval_sorted(int count, typename Fn::T* buf, const uint16_t* list,
+                                                const uint8_t* regs, uint32_t mask) {
   using T = typename Fn::T;
-  const int lane = threadIdx.x & 31;
-  for (int j = lane; j < count; j += 32) {
+  for (int j = threadIdx.x; j < count; j += kBlock) {
     const int li = list[j];
     T v[Fn::NIN], o[Fn::NOUT];
 #pragma unroll
-    for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * kChunk + li];
+    for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * TILE + li];
     Fn::eval(regs[li], v, o, mask);
 #pragma unroll
-    for (int q = 0; q < Fn::NOUT; ++q) buf[q * kChunk + li] = o[q];
+    for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
   }
-  __syncwarp();
-}
-
-template <class Fn>
-__device__ __forceinline__ void warp_slice(unsigned char* base, typename Fn::T*& buf, uint8_t*& list,
-                                           uint8_t*& regs) {
-  using T = typename Fn::T;
-  const int warp = threadIdx.x >> 5;
-  unsigned char* w = base + warp * WarpStage<Fn>::PER_WARP;
-  buf = reinterpret_cast<T*>(w);
-  list = w + (size_t)WarpStage<Fn>::NBUF * kChunk * sizeof(T);
-  regs = list + kChunk;
+  __syncthreads();
 }
 
 template <class Fn, typename TS>
-__global__ void __launch_bounds__(256) map_kernel(const MapParams<Fn::NIN, Fn::NOUT> p) {
+__global__ void __launch_bounds__(kBlock) map_kernel(const MapParams<Fn::NIN, Fn::NOUT> p) {
   using T = typename Fn::T;
+  using S = typename MapTile<Fn>::S;
   constexpr int NIN = Fn::NIN, NOUT = Fn::NOUT, R = Fn::R;
-  const int lane = threadIdx.x & 31;
-  const int64_t nchunks = (p.numel + kChunk - 1) / kChunk;
-  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  constexpr int EPT = S::EPT, TILE = S::TILE;
+  const int tid = threadIdx.x;
+  const int64_t ntiles = (p.numel + TILE - 1) / TILE;
 
   if constexpr (R == 1) {
-    for (int64_t c = wid; c < nchunks; c += nw) {
-      const int64_t base = c * kChunk;
-      T v[kEPT][NIN];
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      T v[EPT][NIN];
 #pragma unroll
-      for (int k = 0; k < kEPT; ++k) {
-        const int64_t i = base + k * 32 + lane;
+      for (int k = 0; k < EPT; ++k) {
+        const int64_t i = t * TILE + k * kBlock + tid;
         if (i < p.numel) load_element<Fn, TS>(p, i, v[k]);
       }
 #pragma unroll
-      for (int k = 0; k < kEPT; ++k) {
-        const int64_t i = base + k * 32 + lane;
+      for (int k = 0; k < EPT; ++k) {
+        const int64_t i = t * TILE + k * kBlock + tid;
         if (i < p.numel) {
           T o[NOUT];
           Fn::eval(0, v[k], o, p.out_mask);
@@ -273,15 +294,17 @@ __global__ void __launch_bounds__(256) map_kernel(const MapParams<Fn::NIN, Fn::N
     }
   } else {
     extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ int s_cnt[R], s_base[R + 1];
     T* buf;
-    uint8_t *list, *regs;
-    warp_slice<Fn>(s_dyn, buf, list, regs);
-    for (int64_t c = wid; c < nchunks; c += nw) {
-      const int64_t base = c * kChunk;
-      int reg[kEPT];
+    uint16_t* list;
+    uint8_t* regs;
+    carve<S>(s_dyn, buf, list, regs);
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const int64_t base = t * TILE;
+      int reg[EPT];
 #pragma unroll
-      for (int k = 0; k < kEPT; ++k) {
-        const int li = k * 32 + lane;
+      for (int k = 0; k < EPT; ++k) {
+        const int li = k * kBlock + tid;
         const int64_t i = base + li;
         reg[k] = R;
         if (i < p.numel) {
@@ -289,125 +312,140 @@ __global__ void __launch_bounds__(256) map_kernel(const MapParams<Fn::NIN, Fn::N
           load_element<Fn, TS>(p, i, v);
           reg[k] = Fn::classify(v);
 #pragma unroll
-          for (int q = 0; q < NIN; ++q) buf[q * kChunk + li] = v[q];
+          for (int q = 0; q < NIN; ++q) buf[q * TILE + li] = v[q];
         }
       }
-      __syncwarp();
-      const int count = warp_sort_by_region<R>(reg, list, regs);
-      warp_eval_sorted<Fn>(count, buf, list, regs, p.out_mask);
+      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base);
+      cta_eval_sorted<Fn, TILE>(count, buf, list, regs, p.out_mask);
 #pragma unroll
-      for (int k = 0; k < kEPT; ++k) {
-        const int li = k * 32 + lane;
+      for (int k = 0; k < EPT; ++k) {
+        const int li = k * kBlock + tid;
         const int64_t i = base + li;
         if (i < p.numel) {
           T o[NOUT];
 #pragma unroll
-          for (int q = 0; q < NOUT; ++q) o[q] = buf[q * kChunk + li];
+          for (int q = 0; q < NOUT; ++q) o[q] = buf[q * TILE + li];
           store_element<Fn, TS>(p, i, o);
         }
       }
-      __syncwarp();
+      __syncthreads();
     }
   }
 }
 
 // ------------------------------------------------------------ 2-D reduction
-// Tiles of kTR rows x 32 columns, one per warp chunk: lane = column, the
-// lane's kEPT elements are the tile's rows.  Row-reduced outputs take a
-// shuffle tree per row, column-reduced outputs a fixed-order sum over the
-// lane's rows; per-tile partials (double) go to the workspace.
+template <class Fn>
+using ReduceStage = Stage<Fn, kTile2D>;
+
 template <class Fn, typename TS>
-__global__ void __launch_bounds__(256) reduce2d_kernel(const Reduce2DParams<Fn::NIN, Fn::NOUT> p) {
+__global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<Fn::NIN, Fn::NOUT> p) {
   using T = typename Fn::T;
+  using S = ReduceStage<Fn>;
   constexpr int NIN = Fn::NIN, NOUT = Fn::NOUT, R = Fn::R;
-  const int lane = threadIdx.x & 31;
-  const int64_t ntiles = p.n_row_tiles * p.n_col_tiles;
-  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  constexpr int EPT = S::EPT, TILE = S::TILE;
+  constexpr int RR = R > 1 ? R : 1;
   extern __shared__ __align__(16) unsigned char s_dyn[];
-  T* buf = nullptr;
-  uint8_t *list = nullptr, *regs = nullptr;
-  if constexpr (R > 1) warp_slice<Fn>(s_dyn, buf, list, regs);
+  __shared__ int s_cnt[RR], s_base[RR + 1];
+  __shared__ double s_red[kBlock / 32][kTC];
+  T* buf;
+  uint16_t* list;
+  uint8_t* regs;
+  carve<S>(s_dyn, buf, list, regs);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t ntiles = p.n_row_tiles * p.n_col_tiles;
 
-  for (int64_t t = wid; t < ntiles; t += nw) {
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t rt = t / p.n_col_tiles, ct = t % p.n_col_tiles;
-    const int64_t r0 = rt * kTR, c = ct * kTC + lane;
-    const bool col_ok = c < p.cols;
-    T res[kEPT][NOUT];
-    bool ok[kEPT];
+    const int64_t r0 = rt * kTR, c0 = ct * kTC;
+    int reg[EPT];
 #pragma unroll
-    for (int k = 0; k < kEPT; ++k) ok[k] = col_ok && (r0 + k) < p.rows;
-
-    if constexpr (R == 1) {
+    for (int k = 0; k < EPT; ++k) {
+      const int li = k * kBlock + tid;
+      const int64_t r = r0 + li / kTC, c = c0 + li % kTC;
+      reg[k] = R;
+      if (r < p.rows && c < p.cols) {
+        T v[NIN];
 #pragma unroll
-      for (int k = 0; k < kEPT; ++k) {
-        if (ok[k]) {
-          T v[NIN];
+        for (int q = 0; q < NIN; ++q)
+          v[q] = load_as<TS, T>(p.in_ptr[q] + (r * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
+        if constexpr (R > 1) reg[k] = Fn::classify(v);
+        else reg[k] = 0;
 #pragma unroll
-          for (int q = 0; q < NIN; ++q)
-            v[q] = load_as<TS, T>(p.in_ptr[q] + ((r0 + k) * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
-          Fn::eval(0, v, res[k], p.out_mask);
-        } else {
-#pragma unroll
-          for (int q = 0; q < NOUT; ++q) res[k][q] = T(0);
-        }
+        for (int q = 0; q < NIN; ++q) buf[q * TILE + li] = v[q];
       }
+    }
+    if constexpr (R > 1) {
+      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base);
+      cta_eval_sorted<Fn, TILE>(count, buf, list, regs, p.out_mask);
     } else {
-      int reg[kEPT];
 #pragma unroll
-      for (int k = 0; k < kEPT; ++k) {
-        const int li = k * 32 + lane;
-        reg[k] = R;
-        if (ok[k]) {
-          T v[NIN];
+      for (int k = 0; k < EPT; ++k) {
+        const int li = k * kBlock + tid;
+        if (reg[k] < R) {
+          T v[NIN], o[NOUT];
 #pragma unroll
-          for (int q = 0; q < NIN; ++q)
-            v[q] = load_as<TS, T>(p.in_ptr[q] + ((r0 + k) * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
-          reg[k] = Fn::classify(v);
+          for (int q = 0; q < NIN; ++q) v[q] = buf[q * TILE + li];
+          Fn::eval(0, v, o, p.out_mask);
 #pragma unroll
-          for (int q = 0; q < NIN; ++q) buf[q * kChunk + li] = v[q];
+          for (int q = 0; q < NOUT; ++q) buf[q * TILE + li] = o[q];
         }
       }
-      __syncwarp();
-      const int count = warp_sort_by_region<R>(reg, list, regs);
-      warp_eval_sorted<Fn>(count, buf, list, regs, p.out_mask);
-#pragma unroll
-      for (int k = 0; k < kEPT; ++k)
-#pragma unroll
-        for (int q = 0; q < NOUT; ++q) res[k][q] = ok[k] ? buf[q * kChunk + k * 32 + lane] : T(0);
-      __syncwarp();
+      __syncthreads();
     }
 
+    const int rows_here = (int)(p.rows - r0 < (int64_t)kTR ? p.rows - r0 : (int64_t)kTR);
+    const int cols_here = (int)(p.cols - c0 < (int64_t)kTC ? p.cols - c0 : (int64_t)kTC);
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
       if (!(p.out_mask & (1u << o))) continue;
       const int kind = p.out_kind[o];
       if (kind == kOutFull) {
 #pragma unroll
-        for (int k = 0; k < kEPT; ++k)
-          if (ok[k])
-            store_as<TS>(p.out_ptr[o] + ((r0 + k) * p.out_s0[o] + c * p.out_s1[o]) * (int64_t)sizeof(TS), res[k][o]);
-      } else if (kind == kOutRow) {
-#pragma unroll
-        for (int k = 0; k < kEPT; ++k) {
-          double v = (double)res[k][o];
+        for (int k = 0; k < EPT; ++k) {
+          const int li = k * kBlock + tid;
+          const int lr = li / kTC, lc = li % kTC;
+          if (lr < rows_here && lc < cols_here)
+            store_as<TS>(p.out_ptr[o] + ((r0 + lr) * p.out_s0[o] + (c0 + lc) * p.out_s1[o]) * (int64_t)sizeof(TS),
+                         buf[o * TILE + li]);
+        }
+      } else if (kind == kOutRow || kind == kOutAll) {
+        // Row sums: warp w takes rows w, w+8, ...; lane = column; fixed
+        // shuffle tree.
+        double tile_sum = 0.0;
+        for (int lr = warp; lr < kTR; lr += kBlock / 32) {
+          double v = (lr < rows_here && lane < cols_here) ? (double)buf[o * TILE + lr * kTC + lane] : 0.0;
 #pragma unroll
           for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-          if (lane == 0 && r0 + k < p.rows) p.ws[o][ct * p.rows + r0 + k] = v;
+          if (kind == kOutRow) {
+            if (lane == 0 && lr < rows_here) p.ws[o][ct * p.rows + r0 + lr] = v;
+          } else {
+            tile_sum += v;
+          }
+        }
+        if (kind == kOutAll) {
+          if (lane == 0) s_red[warp][0] = tile_sum;
+          __syncthreads();
+          if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kBlock / 32; ++w) s += s_red[w][0];
+            p.ws[o][t] = s;
+          }
         }
       } else if (kind == kOutCol) {
+        // Column sums: warp w sums rows w, w+8, ... per lane (= column), then
+        // the warp partials are added in warp order.
         double v = 0.0;
+        for (int lr = warp; lr < rows_here; lr += kBlock / 32) v += (double)buf[o * TILE + lr * kTC + lane];
+        s_red[warp][lane] = v;
+        __syncthreads();
+        if (warp == 0) {
+          double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < kEPT; ++k) v += (double)res[k][o];
-        if (col_ok) p.ws[o][rt * p.cols + c] = v;
-      } else if (kind == kOutAll) {
-        double v = 0.0;
-#pragma unroll
-        for (int k = 0; k < kEPT; ++k) v += (double)res[k][o];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (lane == 0) p.ws[o][t] = v;
+          for (int w = 0; w < kBlock / 32; ++w) s += s_red[w][lane];
+          if (lane < cols_here) p.ws[o][rt * p.cols + c0 + lane] = s;
+        }
       }
+      __syncthreads();
     }
   }
 }
