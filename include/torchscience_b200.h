@@ -125,6 +125,23 @@ TSB_OP_SIGNATURE(tsb_regularized_gamma_q);
 TSB_OP_SIGNATURE(tsb_regularized_gamma_q_backward);
 TSB_OP_SIGNATURE(tsb_regularized_gamma_q_backward_backward);
 
+/* Allocation-free regularized_gamma_p backward (no counterpart in the
+ * reference, whose CPU backward leaves the reduction of broadcast gradients
+ * to the autograd engine).  Same operands and results as
+ * tsb_regularized_gamma_p_backward, but it takes no workspace: for callers
+ * that cannot allocate device memory (hosts reaching this library only
+ * through a C FFI, with no device allocator of their own; loops that must not
+ * call cudaMalloc, which can synchronize the device).  The partial sums of
+ * reduced gradients go to a fixed file-scope device array of
+ * TSB_NOALLOC_SCRATCH_BYTES that each GPU loading the library keeps until
+ * exit; requests needing more return TSB_ERR_WORKSPACE without launching.
+ * The first call on a device looks up the array's address and should come
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be serialized by the caller. */
+#define TSB_NOALLOC_SCRATCH_BYTES (8ll << 20)
+int32_t tsb_regularized_gamma_p_backward_noalloc(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out,
+                                                 int32_t n_out, int32_t precision, void* stream);
+
 /* ---- Complete elliptic integrals --------------------------------------- */
 /* complete_legendre_elliptic_integral_k(m): complete_legendre_elliptic_integral_k.h:29-33,
  * schema torchscience.cpp:1015-1017; backward ..._k_backward.h:24-53,
