@@ -142,6 +142,33 @@ TSB_OP_SIGNATURE(tsb_regularized_gamma_q_backward_backward);
 int32_t tsb_regularized_gamma_p_backward_noalloc(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out,
                                                  int32_t n_out, int32_t precision, void* stream);
 
+/* ---- Bessel functions --------------------------------------------------- */
+/* bessel_j_0(z): bessel_j_0.h:91-129, schema torchscience.cpp:872-874;
+ * backward bessel_j_0_backward.h:27-30, backward_backward bessel_j_0_backward_backward.h:16-30. */
+TSB_OP_SIGNATURE(tsb_bessel_j_0);
+TSB_OP_SIGNATURE(tsb_bessel_j_0_backward);
+TSB_OP_SIGNATURE(tsb_bessel_j_0_backward_backward);
+/* bessel_j(n, z): bessel_j.h:240-316, schema torchscience.cpp:902-904;
+ * backward bessel_j_backward.h:51-63 (grad_n, grad_z), backward_backward bessel_j_backward_backward.h. */
+TSB_OP_SIGNATURE(tsb_bessel_j);
+TSB_OP_SIGNATURE(tsb_bessel_j_backward);
+TSB_OP_SIGNATURE(tsb_bessel_j_backward_backward);
+/* bessel_y(n, z): bessel_y.h:131-193, schema torchscience.cpp:907-909;
+ * backward bessel_y_backward.h:51, backward_backward bessel_y_backward_backward.h. */
+TSB_OP_SIGNATURE(tsb_bessel_y);
+TSB_OP_SIGNATURE(tsb_bessel_y_backward);
+TSB_OP_SIGNATURE(tsb_bessel_y_backward_backward);
+/* modified_bessel_i(n, z): modified_bessel_i.h:271-366, schema torchscience.cpp:917-919;
+ * backward modified_bessel_i_backward.h:51, backward_backward modified_bessel_i_backward_backward.h. */
+TSB_OP_SIGNATURE(tsb_modified_bessel_i);
+TSB_OP_SIGNATURE(tsb_modified_bessel_i_backward);
+TSB_OP_SIGNATURE(tsb_modified_bessel_i_backward_backward);
+/* modified_bessel_k(n, z): modified_bessel_k.h:249-307, schema torchscience.cpp:912-914;
+ * backward modified_bessel_k_backward.h:51, backward_backward modified_bessel_k_backward_backward.h. */
+TSB_OP_SIGNATURE(tsb_modified_bessel_k);
+TSB_OP_SIGNATURE(tsb_modified_bessel_k_backward);
+TSB_OP_SIGNATURE(tsb_modified_bessel_k_backward_backward);
+
 /* ---- Complete elliptic integrals --------------------------------------- */
 /* complete_legendre_elliptic_integral_k(m): complete_legendre_elliptic_integral_k.h:29-33,
  * schema torchscience.cpp:1015-1017; backward ..._k_backward.h:24-53,

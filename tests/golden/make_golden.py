@@ -151,8 +151,36 @@ def elliptic():
     np.savez_compressed(OUT / "elliptic.npz", **d)
 
 
+def bessel():
+    rng = np.random.default_rng(3)
+    n = 3000
+    nu = np.concatenate([rng.uniform(0.0, 20.0, n), rng.uniform(-5.0, 0.0, 300), np.arange(0, 6, dtype=float)])
+    x = np.concatenate([lu(rng, 1e-3, 1e3, n), lu(rng, 1e-2, 50.0, 300), np.full(6, 3.7)])
+    d = {"nu": nu, "x": x, "g": rng.standard_normal(nu.size)}
+    for nm, key in [("bessel_j", "j"), ("bessel_y", "y"), ("modified_bessel_i", "i"), ("modified_bessel_k", "k")]:
+        d[f"ref_{key}"] = ref(nm, 0, nu, x)[0]
+    d["truth_j"], d["truth_y"] = sp.jv(nu, x), sp.yv(nu, x)
+    d["truth_i"], d["truth_k"] = sp.iv(nu, x), sp.kv(nu, x)
+    d["truth_jp"], d["truth_yp"] = sp.jvp(nu, x), sp.yvp(nu, x)
+    d["truth_ip"], d["truth_kp"] = sp.ivp(nu, x), sp.kvp(nu, x)
+    # Near the first 100 zeros of J0 and J1 (config 3 stress set): mpmath truth.
+    z0, z1 = sp.jn_zeros(0, 100), sp.jn_zeros(1, 100)
+    zs = np.concatenate([z0, z1])
+    zn = np.concatenate([np.zeros(100), np.ones(100)])
+    zx = zs * (1.0 + rng.uniform(-1e-6, 1e-6, zs.size))
+    d["zero_nu"], d["zero_x"] = zn, zx
+    d["zero_truth_j"] = np.array([float(mp.besselj(mp.mpf(a), mp.mpf(b))) for a, b in zip(zn, zx)])
+    d["zero_truth_jp"] = np.array([float(mp.besselj(mp.mpf(a), mp.mpf(b), derivative=1)) for a, b in zip(zn, zx)])
+    # ∂/∂ν on a subsample (mpmath).
+    idx = rng.choice(n, 120, replace=False)
+    d["dnu_idx"] = idx
+    d["truth_dnu_j"] = np.array([float(mp.diff(lambda t: mp.besselj(t, mp.mpf(x[i])), mp.mpf(nu[i]))) for i in idx])
+    d["truth_dnu_k"] = np.array([float(mp.diff(lambda t: mp.besselk(t, mp.mpf(x[i])), mp.mpf(nu[i]))) for i in idx])
+    np.savez_compressed(OUT / "bessel.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel"]
     for w in which:
         globals()[w]()
         print("wrote", w)

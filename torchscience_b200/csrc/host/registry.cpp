@@ -263,6 +263,13 @@ TSBH_BINARY_OP(regularized_gamma_p, RegularizedGammaP, a, x, tsb_regularized_gam
                tsb_regularized_gamma_p_backward_backward)
 TSBH_BINARY_OP(regularized_gamma_q, RegularizedGammaQ, a, x, tsb_regularized_gamma_q, tsb_regularized_gamma_q_backward,
                tsb_regularized_gamma_q_backward_backward)
+TSBH_UNARY_OP(bessel_j_0, BesselJ0, z, tsb_bessel_j_0, tsb_bessel_j_0_backward, tsb_bessel_j_0_backward_backward)
+TSBH_BINARY_OP(bessel_j, BesselJ, n, z, tsb_bessel_j, tsb_bessel_j_backward, tsb_bessel_j_backward_backward)
+TSBH_BINARY_OP(bessel_y, BesselY, n, z, tsb_bessel_y, tsb_bessel_y_backward, tsb_bessel_y_backward_backward)
+TSBH_BINARY_OP(modified_bessel_i, ModifiedBesselI, n, z, tsb_modified_bessel_i, tsb_modified_bessel_i_backward,
+               tsb_modified_bessel_i_backward_backward)
+TSBH_BINARY_OP(modified_bessel_k, ModifiedBesselK, n, z, tsb_modified_bessel_k, tsb_modified_bessel_k_backward,
+               tsb_modified_bessel_k_backward_backward)
 TSBH_UNARY_OP(complete_legendre_elliptic_integral_k, CompleteLegendreEllipticIntegralK, m,
               tsb_complete_legendre_elliptic_integral_k, tsb_complete_legendre_elliptic_integral_k_backward,
               tsb_complete_legendre_elliptic_integral_k_backward_backward)

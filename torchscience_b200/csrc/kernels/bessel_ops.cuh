@@ -1,0 +1,278 @@
+// Bessel J_ν, Y_ν, I_ν, K_ν of real order and J_0: functors of the forward,
+// backward (grad_n, grad_z) and double-backward entry points, with the
+// reference's conventions for x <= 0, integer and negative orders
+// (bessel_j.h:240-316, bessel_y.h:131-193, modified_bessel_i.h:271-366,
+// modified_bessel_k.h:249-307, bessel_j_0.h:91-129).
+//
+// ∂/∂x comes with each evaluation; ∂²/∂x² from Bessel's equation.  ∂/∂ν
+// has no practical closed form for real order (the reference also uses
+// central differences, bessel_j_backward.h:17-28); here it is a central
+// difference of the accurate FP64 evaluator with step ε^(1/3)·max(1, |ν|)
+// (ε^(1/4) for the second derivative), only computed when grad_n is
+// requested.
+#pragma once
+
+#include <type_traits>
+
+#include "bessel_math.cuh"
+#include "dispatch.cuh"
+
+namespace tsb {
+
+enum BesselKind : int { kBJ = 0, kBY = 1, kBI = 2, kBK = 3 };
+enum BesselRegion : int { kBsSpecial = 0, kBsSeries = 1, kBsMid = 2, kBsLarge = 3, kBsRegions = 4 };
+
+// Evaluation region (also the unit of compaction).  Mixed kernels run
+// kBsSeries (x < 2, order >= 0 or integer) in FP32 and the others in FP64.
+template <int KIND>
+__device__ __forceinline__ int bessel_classify(double nu, double x) {
+  if (isnan(nu) || isnan(x) || isinf(nu) || isinf(x) || x == 0.0) return kBsSpecial;
+  if ((KIND == kBY || KIND == kBK) && x < 0.0) return kBsSpecial;
+  const double ax = fabs(x), an = fabs(nu);
+  if (ax < 2.0) return (nu >= 0.0 || an == floor(an)) ? kBsSeries : kBsMid;
+  if (ax >= 25.0 && (KIND == kBI || KIND == kBK || an < ax)) return kBsLarge;
+  return kBsMid;
+}
+
+template <typename T>
+struct BV {
+  T v, d;  // value, d/dx
+};
+
+__device__ __forceinline__ bool odd_integer(double a) { return fmod(a, 2.0) == 1.0; }
+__device__ __forceinline__ bool odd_integer(float a) { return fmodf(a, 2.0f) == 1.0f; }
+
+// J_ν(0) / I_ν(0) per the reference (bessel_j.h:253-266, modified_bessel_i.h:278-288).
+template <typename T>
+__device__ __forceinline__ T bessel_at_zero(T nu) {
+  if (nu == T(0)) return T(1);
+  if (nu > T(0)) return T(0);
+  if (nu == floor(nu)) return T(0);
+  return T(CUDART_INF);
+}
+
+template <typename T, int KIND>
+__device__ inline BV<T> bessel_eval(T nu, T x) {
+  const T nan = T(CUDART_NAN), inf = T(CUDART_INF);
+  if (isnan(nu) || isnan(x) || isinf(nu)) return {nan, nan};
+  if (KIND == kBY || KIND == kBK) {
+    if (x < T(0)) return {nan, nan};
+    if (x == T(0)) return KIND == kBY ? BV<T>{-inf, inf} : BV<T>{inf, -inf};
+    if (isinf(x)) return {T(0), T(0)};
+  }
+  const T an = fabs(nu);
+  const bool is_int = an == floor(an);
+  if (x == T(0)) {  // J, I: derivative as (C_{ν-1}(0) ∓ C_{ν+1}(0))/2, like the reference's backward
+    const T c0 = bessel_at_zero(nu), cm = bessel_at_zero(nu - T(1)), cp = bessel_at_zero(nu + T(1));
+    return {c0, KIND == kBJ ? T(0.5) * (cm - cp) : T(0.5) * (cm + cp)};
+  }
+  if (isinf(x)) {
+    if (KIND == kBJ) return {T(0), T(0)};
+    if (x > T(0)) return {inf, inf};
+    if (!is_int) return {nan, nan};
+    const T s = odd_integer(an) ? T(-1) : T(1);
+    return {s * inf, -s * inf};
+  }
+  const T ax = fabs(x);
+  T v, d;
+  if (KIND == kBJ || KIND == kBY) {
+    const bool need_y = KIND == kBY || (nu < T(0) && !is_int);
+    const JY<T> r = need_y ? besseljy_pos<T, true>(an, ax) : besseljy_pos<T, false>(an, ax);
+    if (nu >= T(0) || is_int) {
+      v = KIND == kBJ ? r.j : r.y;
+      d = KIND == kBJ ? r.jp : r.yp;
+      if (nu < T(0) && odd_integer(an)) {  // C_{-n} = (-1)^n C_n
+        v = -v;
+        d = -d;
+      }
+    } else {  // DLMF 10.4.7: J_{-a} = cos(aπ)J_a - sin(aπ)Y_a, Y_{-a} = sin(aπ)J_a + cos(aπ)Y_a
+      T s, c;
+      bx::sincospi_(an, &s, &c);
+      if (KIND == kBJ) {
+        v = c * r.j - s * r.y;
+        d = c * r.jp - s * r.yp;
+      } else {
+        v = s * r.j + c * r.y;
+        d = s * r.jp + c * r.yp;
+      }
+    }
+  } else {
+    bool scaled = false;
+    const bool need_k = KIND == kBK || (nu < T(0) && !is_int);
+    const IK<T> r = KIND == kBK ? besselik_pos<T, false, true>(an, ax, scaled)
+                                : (need_k ? besselik_pos<T, true, true>(an, ax, scaled)
+                                          : besselik_pos<T, true, false>(an, ax, scaled));
+    T i = r.i, ip = r.ip, k = r.k, kp = r.kp;
+    if (scaled) {  // undo e^{-x} I, e^{x} K (split e^x so I does not overflow early)
+      const T eh = bx::exp_(T(0.5) * ax), em = bx::exp_(-ax);
+      i = (i * eh) * eh;
+      ip = (ip * eh) * eh;
+      k *= em;
+      kp *= em;
+    }
+    if (KIND == kBK) {
+      v = k;
+      d = kp;
+    } else if (nu >= T(0) || is_int) {
+      v = i;
+      d = ip;
+    } else {  // DLMF 10.27.2: I_{-a} = I_a + (2/π) sin(aπ) K_a
+      T s, c;
+      bx::sincospi_(an, &s, &c);
+      const T f = T(2) / T(CUDART_PI) * s;
+      v = i + f * k;
+      d = ip + f * kp;
+    }
+  }
+  if (x < T(0)) {  // J, I only: reference sign conventions for negative x
+    T f;
+    if (is_int) {
+      f = odd_integer(an) ? T(-1) : T(1);
+    } else {
+      T s;
+      bx::sincospi_(nu, &s, &f);
+    }
+    v *= f;
+    d = -f * d;
+  }
+  return {v, d};
+}
+
+// Second x-derivative from Bessel's equation (J, Y) or the modified one (I, K).
+template <typename T, int KIND>
+__device__ __forceinline__ T bessel_d2(T nu, T x, const BV<T>& b) {
+  const T r = nu / x;
+  if (KIND == kBJ || KIND == kBY) return -b.d / x - (T(1) - r * r) * b.v;
+  return -b.d / x + (T(1) + r * r) * b.v;
+}
+
+// ν-derivatives by central differences of the FP64 evaluator.
+struct BesselNuDerivs {
+  double dv, dd;  // ∂v/∂ν, ∂(dv/dx)/∂ν
+  double dvv;     // ∂²v/∂ν²
+};
+template <int KIND, bool SECOND>
+__device__ inline BesselNuDerivs bessel_nu_derivs(double nu, double x, const BV<double>& b0) {
+  BesselNuDerivs o;
+  const double h = 6.0554544523933395e-06 * fmax(1.0, fabs(nu));  // ε^(1/3)
+  const BV<double> bp = bessel_eval<double, KIND>(nu + h, x), bm = bessel_eval<double, KIND>(nu - h, x);
+  o.dv = (bp.v - bm.v) / (2.0 * h);
+  o.dd = (bp.d - bm.d) / (2.0 * h);
+  o.dvv = 0.0;
+  if (SECOND) {
+    const double h2 = 1.2207031250e-04 * fmax(1.0, fabs(nu));  // ε^(1/4)
+    const BV<double> cp = bessel_eval<double, KIND>(nu + h2, x), cm = bessel_eval<double, KIND>(nu - h2, x);
+    o.dvv = (cp.v - 2.0 * b0.v + cm.v) / (h2 * h2);
+  }
+  return o;
+}
+
+// Value (+ d/dx): FP32 in the mixed kernels' kBsSeries region, FP64 otherwise;
+// non-finite FP32 results (values at the edge of FP32 range) are redone in FP64.
+template <typename T, int KIND>
+__device__ __forceinline__ BV<T> bessel_value(int region, T nu, T x) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (region == kBsSeries) {
+      const BV<float> f = bessel_eval<float, KIND>(nu, x);
+      if (isfinite(f.v) && isfinite(f.d)) return f;
+    }
+    const BV<double> dd = bessel_eval<double, KIND>((double)nu, (double)x);
+    return {(float)dd.v, (float)dd.d};
+  } else {
+    return bessel_eval<double, KIND>(nu, x);
+  }
+}
+
+template <int KIND, typename T_>
+struct BesselFwd {
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 1, R = kBsRegions;
+  static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return bessel_classify<KIND>((double)in[0], (double)in[1]); }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t) { out[0] = bessel_value<T, KIND>(r, in[0], in[1]).v; }
+};
+
+// in = {grad, n, z}, out = {grad_n, grad_z}
+template <int KIND, typename T_>
+struct BesselBwd {
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = kBsRegions;
+  static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return bessel_classify<KIND>((double)in[1], (double)in[2]); }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t mask) {
+    if (mask & 1u) {  // grad_n needs the FP64 central difference
+      const double nu = in[1], x = in[2], g = in[0];
+      const BV<double> b = bessel_eval<double, KIND>(nu, x);
+      const BesselNuDerivs dn = bessel_nu_derivs<KIND, false>(nu, x, b);
+      out[0] = (T)(g * dn.dv);
+      out[1] = (T)(g * b.d);
+      return;
+    }
+    out[0] = T(0);
+    out[1] = in[0] * bessel_value<T, KIND>(r, in[1], in[2]).d;
+  }
+};
+
+// in = {gg_n, gg_z, grad, n, z}, out = {grad_grad_output, grad_n, grad_z}
+template <int KIND, typename T_>
+struct BesselBwdBwd {
+  using T = T_;
+  static constexpr int NIN = 5, NOUT = 3, R = kBsRegions;
+  static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return bessel_classify<KIND>((double)in[3], (double)in[4]); }
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double ggn = in[0], ggz = in[1], g = in[2], nu = in[3], x = in[4];
+    const BV<double> b = bessel_eval<double, KIND>(nu, x);
+    const BesselNuDerivs dn = bessel_nu_derivs<KIND, true>(nu, x, b);
+    const double d2 = bessel_d2<double, KIND>(nu, x, b);
+    out[0] = (T)(ggn * dn.dv + ggz * b.d);
+    out[1] = (T)(g * (ggn * dn.dvv + ggz * dn.dd));
+    out[2] = (T)(g * (ggn * dn.dd + ggz * d2));
+  }
+};
+
+// J_0 (bessel_j_0): the same evaluator at order 0.
+template <typename T_>
+struct BesselJ0Fwd {
+  using T = T_;
+  static constexpr int NIN = 1, NOUT = 1, R = kBsRegions;
+  static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return bessel_classify<kBJ>(0.0, (double)in[0]); }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t) { out[0] = bessel_value<T, kBJ>(r, T(0), in[0]).v; }
+};
+template <typename T_>
+struct BesselJ0Bwd {  // in = {grad, z}: grad * J0'(z) = -grad * J1(z)
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 1, R = kBsRegions;
+  static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return bessel_classify<kBJ>(0.0, (double)in[1]); }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t) {
+    out[0] = in[0] * bessel_value<T, kBJ>(r, T(0), in[1]).d;
+  }
+};
+template <typename T_>
+struct BesselJ0BwdBwd {  // in = {gg, grad, z}: {gg·J0'(z), gg·grad·J0''(z)}
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = kBsRegions;
+  static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return bessel_classify<kBJ>(0.0, (double)in[2]); }
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double gg = in[0], g = in[1], x = in[2];
+    const BV<double> b = bessel_eval<double, kBJ>(0.0, x);
+    const double d2 = x == 0.0 ? -0.5 : bessel_d2<double, kBJ>(0.0, x, b);
+    out[0] = (T)(gg * b.d);
+    out[1] = (T)(gg * g * d2);
+  }
+};
+
+#define TSB_BESSEL_ALIASES(Name, KIND)                                      \
+  template <typename T> using Name##Fwd = BesselFwd<KIND, T>;              \
+  template <typename T> using Name##Bwd = BesselBwd<KIND, T>;              \
+  template <typename T> using Name##BwdBwd = BesselBwdBwd<KIND, T>;
+
+TSB_BESSEL_ALIASES(BesselJ, kBJ)
+TSB_BESSEL_ALIASES(BesselY, kBY)
+TSB_BESSEL_ALIASES(BesselI, kBI)
+TSB_BESSEL_ALIASES(BesselK, kBK)
+
+}  // namespace tsb

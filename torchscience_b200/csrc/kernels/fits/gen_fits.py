@@ -14,6 +14,10 @@ Fits:
   LGAMMA1P:  lnΓ(1 + a) / a on a in [0, 1], u = 2a - 1 (value -γ at a = 0),
              so lnΓ(1 + a) keeps its absolute accuracy for small a without
              rounding 1 + a.
+  TEMME_G1, TEMME_G2: the Γ combinations of Temme's series for Y_μ, K_μ
+             (|μ| <= 1/2), u = 2μ:
+               g1(μ) = (1/Γ(1-μ) - 1/Γ(1+μ)) / (2μ)   (limit -γ at μ = 0)
+               g2(μ) = (1/Γ(1-μ) + 1/Γ(1+μ)) / 2
 """
 
 from __future__ import annotations
@@ -74,6 +78,18 @@ def lgamma1p_fn(u):
     return mp.loggamma(1 + a) / a
 
 
+def temme_g1(u):
+    mu = u / 2
+    if abs(mu) < mp.mpf("1e-30"):
+        return -mp.euler
+    return (1 / mp.gamma(1 - mu) - 1 / mp.gamma(1 + mu)) / (2 * mu)
+
+
+def temme_g2(u):
+    mu = u / 2
+    return (1 / mp.gamma(1 - mu) + 1 / mp.gamma(1 + mu)) / 2
+
+
 def check(fn, coeffs, lo=-1.0, hi=1.0, n=4001):
     worst = 0.0
     for k in range(n):
@@ -85,7 +101,8 @@ def check(fn, coeffs, lo=-1.0, hi=1.0, n=4001):
 
 
 def emit(name, coeffs, ctype):
-    vals = ", ".join(repr(float(c)) + ("f" if ctype == "float" else "") for c in coeffs)
+    # Coefficients that vanish by symmetry come out ~1e-60; store them as 0.
+    vals = ", ".join(repr(float(c) if abs(c) > 1e-40 else 0.0) + ("f" if ctype == "float" else "") for c in coeffs)
     return f"__device__ constexpr {ctype} {name}[{len(coeffs)}] = {{{vals}}};\n"
 
 
@@ -100,6 +117,10 @@ def main():
     psi_f = cheb_fit(psi_root_fn, 12)
     print("PSI_ROOT double worst rel err", check(psi_root_fn, psi_d))
     print("PSI_ROOT float  worst rel err", check(psi_root_fn, psi_f))
+    g1_d, g2_d = cheb_fit(temme_g1, 22), cheb_fit(temme_g2, 22)
+    g1_f, g2_f = cheb_fit(temme_g1, 10), cheb_fit(temme_g2, 10)
+    print("TEMME_G1 double worst rel err", check(temme_g1, g1_d), "float", check(temme_g1, g1_f))
+    print("TEMME_G2 double worst rel err", check(temme_g2, g2_d), "float", check(temme_g2, g2_f))
     lg1p_d = cheb_fit(lgamma1p_fn, 28)
     print("LGAMMA1P double worst rel err", check(lgamma1p_fn, lg1p_d, hi=0.99))
     text = (
@@ -113,6 +134,11 @@ def main():
         "// psi(x) / (x - x0) on [1, 2] as a polynomial in u = 2x - 3 (ascending powers).\n"
         + emit("PSI_ROOT_D", psi_d, "double")
         + emit("PSI_ROOT_F", psi_f, "float")
+        + "// Temme's g1(μ) = (1/Γ(1-μ) - 1/Γ(1+μ))/(2μ), g2(μ) = (1/Γ(1-μ) + 1/Γ(1+μ))/2, |μ| <= 1/2, in u = 2μ.\n"
+        + emit("TEMME_G1_D", g1_d, "double")
+        + emit("TEMME_G2_D", g2_d, "double")
+        + emit("TEMME_G1_F", g1_f, "float")
+        + emit("TEMME_G2_F", g2_f, "float")
         + "// lnΓ(1 + a) / a on [0, 1] as a polynomial in u = 2a - 1.\n"
         + emit("LGAMMA1P_D", lg1p_d, "double")
         + "\n}  // namespace fits\n}  // namespace tsb\n"

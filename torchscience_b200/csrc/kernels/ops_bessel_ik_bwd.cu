@@ -1,0 +1,5 @@
+// Modified Bessel I_ν, K_ν entry points (bwd); one translation unit per pass keeps builds parallel.
+#include "bessel_ops.cuh"
+
+TSB_DEFINE_OP(tsb_modified_bessel_i_backward, tsb::BesselIBwd)
+TSB_DEFINE_OP(tsb_modified_bessel_k_backward, tsb::BesselKBwd)

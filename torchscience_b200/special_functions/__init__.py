@@ -68,6 +68,48 @@ def complete_legendre_elliptic_integral_k(m: Tensor) -> Tensor:
     return torch.ops.torchscience.complete_legendre_elliptic_integral_k(m)
 
 
+def bessel_j_0(z: Tensor) -> Tensor:
+    """Bessel function of the first kind of order zero J_0(z).
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_bessel_j_0.py).
+    """
+    return torch.ops.torchscience.bessel_j_0(z)
+
+
+def bessel_j(n: Tensor, z: Tensor) -> Tensor:
+    """Bessel function of the first kind J_n(z) of real order n.
+
+    For z < 0 returns (-1)^n J_n(|z|) for integer n and cos(πn) J_n(|z|)
+    otherwise (the reference's real-valued convention).  Same signature and
+    semantics as the reference wrapper (src/torchscience/special_functions/_bessel_j.py:5,193).
+    """
+    return torch.ops.torchscience.bessel_j(n, z)
+
+
+def bessel_y(n: Tensor, z: Tensor) -> Tensor:
+    """Bessel function of the second kind Y_n(z) of real order n; NaN for z < 0, -inf at z = 0.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_bessel_y.py).
+    """
+    return torch.ops.torchscience.bessel_y(n, z)
+
+
+def modified_bessel_i(n: Tensor, z: Tensor) -> Tensor:
+    """Modified Bessel function of the first kind I_n(z) of real order n.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_modified_bessel_i.py).
+    """
+    return torch.ops.torchscience.modified_bessel_i(n, z)
+
+
+def modified_bessel_k(n: Tensor, z: Tensor) -> Tensor:
+    """Modified Bessel function of the second kind K_n(z) of real order n; NaN for z < 0, +inf at z = 0.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_modified_bessel_k.py).
+    """
+    return torch.ops.torchscience.modified_bessel_k(n, z)
+
+
 def complete_legendre_elliptic_integral_e(m: Tensor) -> Tensor:
     """Complete elliptic integral of the second kind E(m) (parameter m = k²); NaN for m > 1, E(1) = 1.
 
@@ -76,4 +118,10 @@ def complete_legendre_elliptic_integral_e(m: Tensor) -> Tensor:
     return torch.ops.torchscience.complete_legendre_elliptic_integral_e(m)
 
 
-__all__ = ["complete_legendre_elliptic_integral_e", "complete_legendre_elliptic_integral_k", "digamma", "gamma", "log_gamma", "regularized_gamma_p", "regularized_gamma_q", "trigamma"]
+__all__ = [
+    "bessel_j",
+    "bessel_j_0",
+    "bessel_y",
+    "modified_bessel_i",
+    "modified_bessel_k",
+   "complete_legendre_elliptic_integral_e", "complete_legendre_elliptic_integral_k", "digamma", "gamma", "log_gamma", "regularized_gamma_p", "regularized_gamma_q", "trigamma"]
