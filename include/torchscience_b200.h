@@ -169,6 +169,17 @@ TSB_OP_SIGNATURE(tsb_modified_bessel_k);
 TSB_OP_SIGNATURE(tsb_modified_bessel_k_backward);
 TSB_OP_SIGNATURE(tsb_modified_bessel_k_backward_backward);
 
+/* ---- Gauss hypergeometric function ----------------------------------- */
+/* hypergeometric_2_f_1(a, b, c, z) for real arguments: hypergeometric_2_f_1.h:203-295,
+ * schema torchscience.cpp:837-839; backward hypergeometric_2_f_1_backward.h:60-118
+ * (outputs grad_a, grad_b, grad_c, grad_z), backward_backward
+ * hypergeometric_2_f_1_backward_backward.h:12-125 (inputs gg_a, gg_b, gg_c, gg_z,
+ * grad_output, a, b, c, z; outputs gg_out, grad_a, grad_b, grad_c, grad_z).
+ * Every precision mode evaluates in FP64. */
+TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1);
+TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1_backward);
+TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1_backward_backward);
+
 /* ---- Complete elliptic integrals --------------------------------------- */
 /* complete_legendre_elliptic_integral_k(m): complete_legendre_elliptic_integral_k.h:29-33,
  * schema torchscience.cpp:1015-1017; backward ..._k_backward.h:24-53,

@@ -4,7 +4,10 @@
  * A plain-C restatement of the reference's scalar algorithms for the part of
  * the accelerated path whose reference implementation is short and accurate:
  * lnΓ, Γ, ψ, ψ', ψ'', ψ''', the regularized incomplete gamma P/Q (forward and
- * backward) and the complete elliptic integrals K, E (forward).  Each function
+ * backward), the complete elliptic integrals K, E (forward) and the Gauss
+ * hypergeometric 2F1 for real arguments (forward, backward and
+ * backward_backward, including the reference's unconverged series for
+ * 1/2 <= z < 1 and its finite-difference derivatives).  Each function
  * cites the reference file:line it restates
  * (paths under src/torchscience/csrc/kernel/special_functions/).  Operation
  * order follows the reference so that, with the same libm, results agree with
@@ -12,14 +15,16 @@
  * of the reference itself (tests/golden/reference_*.npz, made by
  * tests/golden/make_golden.py from oracle/_ref/libref_scalar.so).
  *
- * Bessel J/Y/I/K of real order and 2F1 are not restated here: their parity is
+ * Bessel J/Y/I/K of real order are not restated here: their parity is
  * anchored on the reference's compiled code (oracle/_ref) and on scipy/mpmath
  * fixtures, because the reference is inaccurate over large parts of their
- * domains (documented reference-defect bands).
+ * domains (documented reference-defect bands).  For 2F1 the restatement fixes
+ * the reference's special-case semantics; accuracy is judged against mpmath.
  *
  * ABI: int oracle_eval(const char* name, int pass, const double* const* in,
  *                      double* const* out, int64_t n)
- * pass 0 = forward, 1 = backward; returns 0 or -1 (unknown name/pass).
+ * pass 0 = forward, 1 = backward, 2 = backward_backward (2F1 only); returns 0
+ * or -1 (unknown name/pass).
  */
 #include <math.h>
 #include <stdint.h>
@@ -238,6 +243,145 @@ static double ref_rg(double x, double y, double z) {
 static double ref_ellip_k(double m) { return ref_rf(0.0, 1.0 - m, 1.0); }
 static double ref_ellip_e(double m) { return 2.0 * ref_rg(0.0, 1.0 - m, 1.0); }
 
+/* ---- Gauss 2F1, real arguments (hypergeometric_2_f_1.h) ----------------- */
+#define H2_EPS 1e-15 /* hyp2f1_epsilon<double>, :38-47 */
+
+static int h2_nonpos(double x) { return x <= 0.0 && fabs(x - round(x)) < H2_EPS; } /* :49-62 */
+static int h2_int(double x) { return (int)round(x); }                            /* :64-73 */
+
+/* :75-94: the series, stopping on a vanishing (c + n)(n + 1) or a term below eps |sum| */
+static double h2_series(double a, double b, double c, double z, int max_iter) {
+  double sum = 1.0, term = 1.0;
+  for (int n = 0; n < max_iter; ++n) {
+    const double denom = (c + (double)n) * (double)(n + 1);
+    if (fabs(denom) < H2_EPS) break;
+    term *= (a + (double)n) * (b + (double)n) / denom * z;
+    sum += term;
+    if (fabs(term) < H2_EPS * fabs(sum)) return sum;
+  }
+  return sum;
+}
+
+/* :96-116 (for real 1/2 <= z < 1, |z/(z-1)| >= 1: always the 2000-term series) */
+static double h2_near_one(double a, double b, double c, double z) {
+  const double zt = z / (z - 1.0);
+  if (fabs(zt) < 0.5) return pow(1.0 - z, -a) * h2_series(a, c - b, c, zt, 500);
+  if (fabs(zt) < 0.9) return pow(1.0 - z, -b) * h2_series(b, c - a, c, zt, 500);
+  return h2_series(a, b, c, z, 2000);
+}
+
+/* :118-149 */
+static double h2_at_one(double a, double b, double c) {
+  const double s = c - a - b;
+  if (s <= 0.0) return NAN;
+  return tgamma(c) * tgamma(s) / (tgamma(c - a) * tgamma(c - b));
+}
+
+/* :151-163 */
+static double h2_negative_z(double a, double b, double c, double z) {
+  const double w = z / (z - 1.0);
+  const double pre = pow(1.0 - z, -a);
+  if (fabs(w) < 0.5) return pre * h2_series(a, c - b, c, w, 500);
+  return pre * h2_series(a, c - b, c, w, 1000);
+}
+
+/* :203-295 */
+static double ref_hyp2f1(double a, double b, double c, double z) {
+  if (fabs(z) < H2_EPS) return 1.0;
+  if (fabs(a) < H2_EPS || fabs(b) < H2_EPS) return 1.0;
+  if (h2_nonpos(c)) {
+    const int ci = h2_int(c);
+    const int a_cancels = h2_nonpos(a) && h2_int(a) > ci;
+    const int b_cancels = h2_nonpos(b) && h2_int(b) > ci;
+    if (!a_cancels && !b_cancels) return INFINITY;
+  }
+  /* :165-198: the series diverges on |z| = 1, z != 1, when c - a - b <= -1 */
+  if (fabs(fabs(z) - 1.0) < 1e-10 && !(fabs(z - 1.0) < 1e-10) && c - a - b <= -1.0) return NAN;
+  if (fabs(c - b) < H2_EPS) return pow(1.0 - z, -a);
+  if (fabs(c - a) < H2_EPS) return pow(1.0 - z, -b);
+  if (h2_nonpos(a)) return h2_series(a, b, c, z, -h2_int(a) + 1);
+  if (h2_nonpos(b)) return h2_series(a, b, c, z, -h2_int(b) + 1);
+  if (fabs(z - 1.0) < 1e-10) return h2_at_one(a, b, c);
+  if (z < 0.0) return h2_negative_z(a, b, c, z);
+  if (fabs(z) < 0.5) return h2_series(a, b, c, z, 500);
+  if (fabs(z) < 1.0) return h2_near_one(a, b, c, z);
+  return NAN;
+}
+
+/* hypergeometric_2_f_1_backward.h:20-56: the series with its parameter derivatives */
+static void h2_series_grads(double a, double b, double c, double z, double* da, double* db, double* dc) {
+  double sum = 1.0, term = 1.0, ha = 0.0, hb = 0.0, hc = 0.0;
+  *da = *db = *dc = 0.0;
+  for (int n = 0; n < 500; ++n) {
+    if (n > 0) {
+      ha += 1.0 / (a + (double)(n - 1));
+      hb += 1.0 / (b + (double)(n - 1));
+      hc += 1.0 / (c + (double)(n - 1));
+      *da += term * ha;
+      *db += term * hb;
+      *dc -= term * hc;
+    }
+    const double denom = (c + (double)n) * (double)(n + 1);
+    if (fabs(denom) < H2_EPS) break;
+    term *= (a + (double)n) * (b + (double)n) / denom * z;
+    sum += term;
+    if (fabs(term) < H2_EPS * fabs(sum)) break;
+  }
+}
+
+/* hypergeometric_2_f_1_backward.h:60-118: analytic for |z| < 1/2 (a, b not
+ * non-positive integers), central differences with step sqrt(eps) otherwise */
+static void ref_hyp2f1_backward(double g, double a, double b, double c, double z, double* o) {
+  const double dfdz = (a * b / c) * ref_hyp2f1(a + 1.0, b + 1.0, c + 1.0, z);
+  double dfda, dfdb, dfdc;
+  if (fabs(z) < 0.5 && !h2_nonpos(a) && !h2_nonpos(b)) {
+    h2_series_grads(a, b, c, z, &dfda, &dfdb, &dfdc);
+  } else {
+    const double e = sqrt(H2_EPS);
+    dfda = (ref_hyp2f1(a + e, b, c, z) - ref_hyp2f1(a - e, b, c, z)) / (2.0 * e);
+    dfdb = (ref_hyp2f1(a, b + e, c, z) - ref_hyp2f1(a, b - e, c, z)) / (2.0 * e);
+    dfdc = (ref_hyp2f1(a, b, c + e, z) - ref_hyp2f1(a, b, c - e, z)) / (2.0 * e);
+  }
+  o[0] = g * dfda;
+  o[1] = g * dfdb;
+  o[2] = g * dfdc;
+  o[3] = g * dfdz;
+}
+
+/* hypergeometric_2_f_1_backward_backward.h:12-125: differences with step eps^(1/4) */
+static void ref_hyp2f1_backward_backward(double gga, double ggb, double ggc, double ggz, double g, double a, double b,
+                                         double c, double z, double* o) {
+  const double dz_coef = a * b / c;
+  const double d2z_coef = dz_coef * (a + 1.0) * (b + 1.0) / (c + 1.0);
+  const double f1 = ref_hyp2f1(a + 1.0, b + 1.0, c + 1.0, z);
+  const double f2 = ref_hyp2f1(a + 2.0, b + 2.0, c + 2.0, z);
+  const double e = pow(H2_EPS, 0.25);
+  const double df_da = (ref_hyp2f1(a + e, b, c, z) - ref_hyp2f1(a - e, b, c, z)) / (2.0 * e);
+  const double df_db = (ref_hyp2f1(a, b + e, c, z) - ref_hyp2f1(a, b - e, c, z)) / (2.0 * e);
+  const double df_dc = (ref_hyp2f1(a, b, c + e, z) - ref_hyp2f1(a, b, c - e, z)) / (2.0 * e);
+  const double df_dz = dz_coef * f1;
+  const double gg_out = gga * df_da + ggb * df_db + ggc * df_dc + ggz * df_dz;
+  const double d2f_dz2 = d2z_coef * f2;
+  double ap[4], am[4], bp[4], bm[4], cp[4], cm[4], zp[4], zm[4];
+  ref_hyp2f1_backward(1.0, a + e, b, c, z, ap);
+  ref_hyp2f1_backward(1.0, a - e, b, c, z, am);
+  ref_hyp2f1_backward(1.0, a, b + e, c, z, bp);
+  ref_hyp2f1_backward(1.0, a, b - e, c, z, bm);
+  ref_hyp2f1_backward(1.0, a, b, c + e, z, cp);
+  ref_hyp2f1_backward(1.0, a, b, c - e, z, cm);
+  ref_hyp2f1_backward(1.0, a, b, c, z + e, zp);
+  ref_hyp2f1_backward(1.0, a, b, c, z - e, zm);
+  const double h = 2.0 * e;
+  const double d2a = (ap[0] - am[0]) / h, d2b = (bp[1] - bm[1]) / h, d2c = (cp[2] - cm[2]) / h;
+  const double dab = (bp[0] - bm[0]) / h, dac = (cp[0] - cm[0]) / h, dbc = (cp[1] - cm[1]) / h;
+  const double daz = (zp[0] - zm[0]) / h, dbz = (zp[1] - zm[1]) / h, dcz = (zp[2] - zm[2]) / h;
+  o[0] = gg_out;
+  o[1] = g * (gga * d2a + ggb * dab + ggc * dac + ggz * daz);
+  o[2] = g * (gga * dab + ggb * d2b + ggc * dbc + ggz * dbz);
+  o[3] = g * (gga * dac + ggb * dbc + ggc * d2c + ggz * dcz);
+  o[4] = g * (gga * daz + ggb * dbz + ggc * dcz + ggz * d2f_dz2);
+}
+
 #define UNARY_FWD(nm, fn)                                           \
   if (strcmp(name, nm) == 0 && pass == 0) {                         \
     _Pragma("omp parallel for schedule(dynamic, 256)")              \
@@ -282,6 +426,32 @@ int oracle_eval(const char* name, int pass, const double* const* in, double* con
       out[0][i] = in[0][i] * d;
     }
     return 0;
+  }
+  if (strcmp(name, "hypergeometric_2_f_1") == 0) {
+    if (pass == 0) {
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t i = 0; i < n; ++i) out[0][i] = ref_hyp2f1(in[0][i], in[1][i], in[2][i], in[3][i]);
+      return 0;
+    }
+    if (pass == 1) {
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t i = 0; i < n; ++i) {
+        double o[4];
+        ref_hyp2f1_backward(in[0][i], in[1][i], in[2][i], in[3][i], in[4][i], o);
+        for (int k = 0; k < 4; ++k) out[k][i] = o[k];
+      }
+      return 0;
+    }
+    if (pass == 2) {
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t i = 0; i < n; ++i) {
+        double o[5];
+        ref_hyp2f1_backward_backward(in[0][i], in[1][i], in[2][i], in[3][i], in[4][i], in[5][i], in[6][i], in[7][i],
+                                     in[8][i], o);
+        for (int k = 0; k < 5; ++k) out[k][i] = o[k];
+      }
+      return 0;
+    }
   }
   return -1;
 }

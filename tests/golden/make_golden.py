@@ -6,7 +6,7 @@ fixtures):
     python oracle/build_ref.py && python tests/golden/make_golden.py
 
 Each fixture holds seeded inputs drawn from the distributions of the
-benchmark configurations (SURVEY/BASELINE configs, small samples), the
+benchmark configurations (small samples), the
 reference's own outputs for them (oracle/_ref/libref_scalar.so, i.e. the
 reference's scalar templates compiled from its sources) and high-accuracy
 values from scipy 1.18 / mpmath 1.3 ("truth").
@@ -179,8 +179,76 @@ def bessel():
     np.savez_compressed(OUT / "bessel.npz", **d)
 
 
+def hyp2f1():
+    """2F1 fixtures: the reference's known answers, its scipy grid, a seeded
+    sample of the benchmark distribution (a, b, c ~ U(-10, 10), c rejected
+    within 1e-3 of a non-positive integer, z ~ U(-5, 0.9) w.p. 0.9 else
+    U(0.9, 0.999)) with mpmath values, gradients and input condition numbers
+    κ = Σ|x_i ∂F/∂x_i| / |F|, Hessians on a subsample, and the reference's
+    outputs on its special points."""
+    rng = np.random.default_rng(4)
+    d = {}
+    # Known answers, test__hypergeometric_2_f_1.py:2604-2703.
+    kat = [(1.5, 2.5, 3.5, 0.3, 1.452767637957694), (-2.0, 3.0, 4.0, 0.7, 0.244), (1.0, 2.0, -1.0, 0.3, np.inf),
+           (2.0, 3.0, 3.0, 0.3, 0.7 ** -2.0), (1.0, 2.0, 4.0, 0.9, 2.1789423102929675),
+           (1.0, 2.0, 3.0, -5.0, 0.2566592424617554), (1.5, 2.5, 3.5, -2.0, 0.28453773594866716)]
+    d["kat"] = np.array(kat)
+    # The scipy grid of test__hypergeometric_2_f_1.py:327-345 and the z -> 1 sweep of :1944-1970.
+    g = np.array([(a, b, c, z) for z in (0.1, 0.3, 0.5, 0.7) for a in (0.5, 1.0, 2.0) for b in (0.5, 1.0, 2.0)
+                  for c in (1.0, 2.0, 3.0)] + [(0.3, 0.4, 2.0, z) for z in (0.99, 0.999, 0.9999, 0.99999)])
+    d["grid"] = g
+    d["grid_truth"] = np.array([float(mp.hyp2f1(*map(mp.mpf, r))) for r in g])
+    # Integer c - a - b near z = 1 and z -> -inf (the degenerate connection formula).
+    deg = np.array([(1.0, 2.0, 4.0, 0.999), (1.0, 2.0, 4.0, 0.9999), (1.0, 2.0, 3.0, 0.9995), (0.5, 1.5, 3.0, 0.9999),
+                    (2.5, 1.5, 5.0, 0.99999), (1.0, 2.0, 3.0, -500.0), (1.5, 1.5, 2.0, -300.0)])
+    d["degenerate"] = deg
+    d["degenerate_truth"] = np.array([float(mp.hyp2f1(*map(mp.mpf, r))) for r in deg])
+    # Benchmark-distribution sample.
+    n = 1500
+    a = rng.uniform(-10, 10, n)
+    b = rng.uniform(-10, 10, n)
+    c = rng.uniform(-10, 10, n)
+    bad = (c <= 0) & (np.abs(c - np.round(c)) < 1e-3)
+    while bad.any():
+        c[bad] = rng.uniform(-10, 10, bad.sum())
+        bad = (c <= 0) & (np.abs(c - np.round(c)) < 1e-3)
+    z = np.where(rng.random(n) < 0.9, rng.uniform(-5, 0.9, n), rng.uniform(0.9, 0.999, n))
+    d["a"], d["b"], d["c"], d["z"] = a, b, c, z
+    d["ref"] = ref("hypergeometric_2_f_1", 0, a, b, c, z)[0]
+    f = lambda A, B, C, Z: mp.hyp2f1(A, B, C, Z)  # noqa: E731
+    truth, grad, kappa = np.empty(n), np.empty((n, 4)), np.empty(n)
+    for i in range(n):
+        X = [mp.mpf(v) for v in (a[i], b[i], c[i], z[i])]
+        F = f(*X)
+        gi = [mp.diff(f, X, tuple(int(j == k) for j in range(4))) for k in range(4)]
+        truth[i] = float(F)
+        grad[i] = [float(v) for v in gi]
+        kappa[i] = float(sum(abs(X[k] * gi[k]) for k in range(4)) / abs(F))
+    d["truth"], d["truth_grad"], d["kappa"] = truth, grad, kappa
+    m = 300
+    d["g"] = rng.standard_normal(m)
+    d["ref_grad"] = np.stack(ref("hypergeometric_2_f_1", 1, d["g"], a[:m], b[:m], c[:m], z[:m]), axis=1)
+    # Hessians [aa, ab, ac, az, bb, bc, bz, cc, cz, zz] on the first 60 points.
+    pairs = [(0, 0), (0, 1), (0, 2), (0, 3), (1, 1), (1, 2), (1, 3), (2, 2), (2, 3), (3, 3)]
+    hess = np.empty((60, 10))
+    for i in range(60):
+        X = [mp.mpf(v) for v in (a[i], b[i], c[i], z[i])]
+        hess[i] = [float(mp.diff(f, X, tuple(int(p == j) + int(q == j) for j in range(4)))) for p, q in pairs]
+    d["truth_hess"] = hess
+    # Special points: the reference's early returns and their neighbourhoods.
+    sp_pts = [(0.0, 2.0, 3.0, 0.4), (1.5, 0.0, 3.0, -2.0), (1.5, 2.5, 3.5, 0.0), (2.0, 1.5, 1.5, -0.7),
+              (1.5, 2.0, 1.5, 0.6), (-3.0, 2.5, 4.5, 0.8), (2.5, -4.0, 1.5, -3.0), (-1.0, 2.0, -2.0, 0.5),
+              (-3.0, 2.0, -2.0, 0.5), (1.0, 2.0, -3.0, 0.5), (0.5, 0.25, 2.0, 1.0), (1.5, 2.5, 3.0, 1.0),
+              (2.0, 3.0, 3.5, -1.0), (0.5, 0.5, 3.0, -1.0), (1.0, 2.0, 3.0, 1.5), (1.0, 2.0, 3.0, np.nan),
+              (np.nan, 2.0, 3.0, 0.5), (1.0, 2.0, 3.0, -1e-16), (1.2, 2.3, 3.4, 0.5), (1.2, 2.3, 3.4, -1.0 - 1e-12)]
+    sp_pts = np.array(sp_pts)
+    d["special"] = sp_pts
+    d["special_ref"] = ref("hypergeometric_2_f_1", 0, *sp_pts.T)[0]
+    np.savez_compressed(OUT / "hyp2f1.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "hyp2f1"]
     for w in which:
         globals()[w]()
         print("wrote", w)

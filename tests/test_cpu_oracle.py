@@ -85,3 +85,41 @@ def test_reference_accuracy_bands():
     assert rel_err(el["ref_k"], el["truth_k"])[inside].max() < 1e-13
     # E(1) and m -> 1 are where the reference's R_G form loses accuracy
     assert rel_err(el["ref_e"], el["truth_e"])[inside].max() < 1e-12
+
+
+def _same(x, y):
+    return bool(np.all((x == y) | (np.isnan(x) & np.isnan(y))))
+
+
+def test_restatement_matches_reference_outputs_hyp2f1():
+    """The 2F1 restatement is bit-identical to the reference's compiled scalar
+    kernel: forward on the benchmark sample and the special points, backward
+    (analytic and finite-difference branches) on its first 300 points."""
+    d = golden("hyp2f1")
+    assert _same(O.restated("hypergeometric_2_f_1", 0, d["a"], d["b"], d["c"], d["z"])[0], d["ref"])
+    sp = d["special"]
+    assert _same(O.restated("hypergeometric_2_f_1", 0, *sp.T)[0], d["special_ref"])
+    m = d["g"].size
+    got = O.restated("hypergeometric_2_f_1", 1, d["g"], d["a"][:m], d["b"][:m], d["c"][:m], d["z"][:m], n_out=4)
+    for k in range(4):
+        assert _same(got[k], d["ref_grad"][:, k])
+
+
+def test_hyp2f1_known_answers_from_reference_tests():
+    """test__hypergeometric_2_f_1.py:2604-2703 (scipy values, tolerances as there)."""
+    k = golden("hyp2f1")["kat"]
+    got = O.restated("hypergeometric_2_f_1", 0, *k[:, :4].T)[0]
+    fin = np.isfinite(k[:, 4])
+    np.testing.assert_allclose(got[fin], k[fin, 4], rtol=1e-8, atol=1e-8)
+    assert np.isposinf(got[~fin]).all()
+
+
+def test_hyp2f1_reference_accuracy_bands():
+    """The reference is accurate for z < 1/2 away from cancellation and wrong
+    near z = 1, where its 2000-term series has not converged."""
+    d = golden("hyp2f1")
+    e = rel_err(d["ref"], d["truth"])
+    z = d["z"]
+    assert np.median(e[z < 0.5]) < 1e-14
+    assert e[z >= 0.95].max() > 1e-3
+    assert np.median(e[z >= 0.99]) > 1e-8

@@ -20,7 +20,7 @@ OPS_LIBRARY = _os.path.join(_HERE, "libtsb_ops.so")
 if not (_os.path.exists(KERNEL_LIBRARY) and _os.path.exists(OPS_LIBRARY)):
     raise ImportError(
         "torchscience_b200 native libraries are not built "
-        f"(expected {OPS_LIBRARY}); run `python -m torchscience_b200._build`"
+        f"(expected {OPS_LIBRARY}); run `python torchscience_b200/_build.py`"
     )
 
 _torch.ops.load_library(OPS_LIBRARY)

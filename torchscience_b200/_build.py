@@ -5,7 +5,7 @@ libtsb_cuda.so  the sm_100a kernels behind the C ABI in include/torchscience_b20
 libtsb_ops.so   the torch.ops.torchscience registration (CUDA / Meta / Autograd /
                 AutocastCUDA / CPU-error kernels) that calls the C ABI.
 
-Usage: python -m torchscience_b200._build [--force] [-j N]
+Usage: python torchscience_b200/_build.py [--force] [-j N]
 """
 
 from __future__ import annotations

@@ -277,6 +277,156 @@ TSBH_UNARY_OP(complete_legendre_elliptic_integral_e, CompleteLegendreEllipticInt
               tsb_complete_legendre_elliptic_integral_e, tsb_complete_legendre_elliptic_integral_e_backward,
               tsb_complete_legendre_elliptic_integral_e_backward_backward)
 
+// ------------------------------------------------------------ 2F1(a, b; c; z)
+// The one quaternary op (reference CPU loop: cpu/macros.h:2905; autograd
+// structure as the binary ops above, with four inputs).
+namespace tsbh::ops {
+using T4 = std::tuple<at::Tensor, at::Tensor, at::Tensor, at::Tensor>;
+using T5 = std::tuple<at::Tensor, at::Tensor, at::Tensor, at::Tensor, at::Tensor>;
+
+at::Tensor hyp2f1_cuda(const at::Tensor& a, const at::Tensor& b, const at::Tensor& c, const at::Tensor& z) {
+  return run_pointwise(tsb_hypergeometric_2_f_1, "hypergeometric_2_f_1", {a, b, c, z}, 1)[0];
+}
+T4 hyp2f1_backward_cuda(const at::Tensor& g, const at::Tensor& a, const at::Tensor& b, const at::Tensor& c,
+                        const at::Tensor& z) {
+  auto r = run_pointwise(tsb_hypergeometric_2_f_1_backward, "hypergeometric_2_f_1_backward", {g, a, b, c, z}, 4);
+  return {r[0], r[1], r[2], r[3]};
+}
+T5 hyp2f1_backward_backward_cuda(const at::Tensor& gga, const at::Tensor& ggb, const at::Tensor& ggc,
+                                 const at::Tensor& ggz, const at::Tensor& g, const at::Tensor& a, const at::Tensor& b,
+                                 const at::Tensor& c, const at::Tensor& z) {
+  auto r = run_pointwise(tsb_hypergeometric_2_f_1_backward_backward, "hypergeometric_2_f_1_backward_backward",
+                         {gga, ggb, ggc, ggz, g, a, b, c, z}, 5);
+  return {r[0], r[1], r[2], r[3], r[4]};
+}
+at::Tensor hyp2f1_meta(const at::Tensor& a, const at::Tensor& b, const at::Tensor& c, const at::Tensor& z) {
+  return meta_pointwise("hypergeometric_2_f_1", {a, b, c, z}, 1)[0];
+}
+T4 hyp2f1_backward_meta(const at::Tensor& g, const at::Tensor& a, const at::Tensor& b, const at::Tensor& c,
+                        const at::Tensor& z) {
+  auto r = meta_pointwise("hypergeometric_2_f_1_backward", {g, a, b, c, z}, 4);
+  return {r[0], r[1], r[2], r[3]};
+}
+T5 hyp2f1_backward_backward_meta(const at::Tensor& gga, const at::Tensor& ggb, const at::Tensor& ggc,
+                                 const at::Tensor& ggz, const at::Tensor& g, const at::Tensor& a, const at::Tensor& b,
+                                 const at::Tensor& c, const at::Tensor& z) {
+  auto r = meta_pointwise("hypergeometric_2_f_1_backward_backward", {gga, ggb, ggc, ggz, g, a, b, c, z}, 5);
+  return {r[0], r[1], r[2], r[3], r[4]};
+}
+at::Tensor hyp2f1_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&) {
+  cpu_not_supported("hypergeometric_2_f_1");
+}
+T4 hyp2f1_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                       const at::Tensor&) {
+  cpu_not_supported("hypergeometric_2_f_1_backward");
+}
+T5 hyp2f1_backward_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                const at::Tensor&) {
+  cpu_not_supported("hypergeometric_2_f_1_backward_backward");
+}
+
+class Hypergeometric2F1Backward : public torch::autograd::Function<Hypergeometric2F1Backward> {
+ public:
+  static variable_list forward(AutogradContext* ctx, const at::Tensor& g, const at::Tensor& a, const at::Tensor& b,
+                               const at::Tensor& c, const at::Tensor& z, std::vector<bool> want) {
+    ctx->save_for_backward({g, a, b, c, z});
+    for (int i = 0; i < 4; ++i) ctx->saved_data["r" + std::to_string(i)] = static_cast<bool>(want[i]);
+    at::AutoDispatchBelowAutograd guard;
+    if (any_cuda({g, a, b, c, z})) {
+      /* Gradients come back already reduced to the inputs' shapes. */
+      return run_reduced_backward(tsb_hypergeometric_2_f_1_backward, "hypergeometric_2_f_1_backward", g,
+                                  {a, b, c, z}, want);
+    }
+    static auto op = c10::Dispatcher::singleton()
+                         .findSchemaOrThrow("torchscience::hypergeometric_2_f_1_backward", "")
+                         .typed<T4(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                   const at::Tensor&)>();
+    auto [ga, gb, gc, gz] = op.call(g, a, b, c, z);
+    return {ga, gb, gc, gz};
+  }
+  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
+    auto saved = ctx->get_saved_variables();
+    bool any_req = false, any_go = false;
+    for (int i = 0; i < 4; ++i) {
+      any_req = any_req || ctx->saved_data["r" + std::to_string(i)].toBool();
+      any_go = any_go || go[i].defined();
+    }
+    variable_list none(7);
+    if (!any_go || !any_req) return none;
+    at::AutoDispatchBelowAutograd guard;
+    at::Tensor gg[4];
+    for (int i = 0; i < 4; ++i) gg[i] = go[i].defined() ? go[i] : at::zeros_like(saved[1 + i]);
+    static auto op = c10::Dispatcher::singleton()
+                         .findSchemaOrThrow("torchscience::hypergeometric_2_f_1_backward_backward", "")
+                         .typed<T5(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                   const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                   const at::Tensor&)>();
+    auto [gg_out, g_a, g_b, g_c, g_z] =
+        op.call(gg[0], gg[1], gg[2], gg[3], saved[0], saved[1], saved[2], saved[3], saved[4]);
+    return {gg_out, g_a, g_b, g_c, g_z, at::Tensor()};
+  }
+};
+
+class Hypergeometric2F1 : public torch::autograd::Function<Hypergeometric2F1> {
+ public:
+  static at::Tensor forward(AutogradContext* ctx, const at::Tensor& a, const at::Tensor& b, const at::Tensor& c,
+                            const at::Tensor& z) {
+    ctx->save_for_backward({a, b, c, z});
+    const at::Tensor* in[4] = {&a, &b, &c, &z};
+    for (int i = 0; i < 4; ++i) ctx->saved_data["r" + std::to_string(i)] = wants_grad(*in[i]);
+    at::AutoDispatchBelowAutograd guard;
+    static auto op = c10::Dispatcher::singleton()
+                         .findSchemaOrThrow("torchscience::hypergeometric_2_f_1", "")
+                         .typed<at::Tensor(const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                           const at::Tensor&)>();
+    return op.call(a, b, c, z);
+  }
+  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
+    auto saved = ctx->get_saved_variables();
+    std::vector<bool> want(4);
+    for (int i = 0; i < 4; ++i) want[i] = ctx->saved_data["r" + std::to_string(i)].toBool();
+    auto g = Hypergeometric2F1Backward::apply(go[0], saved[0], saved[1], saved[2], saved[3], want);
+    variable_list out(4);
+    for (int i = 0; i < 4; ++i) out[i] = want[i] ? g[i] : at::Tensor();
+    return out;
+  }
+};
+
+at::Tensor hyp2f1_autograd(const at::Tensor& a, const at::Tensor& b, const at::Tensor& c, const at::Tensor& z) {
+  return Hypergeometric2F1::apply(a, b, c, z);
+}
+at::Tensor hyp2f1_autocast(const at::Tensor& a, const at::Tensor& b, const at::Tensor& c, const at::Tensor& z) {
+  c10::impl::ExcludeDispatchKeyGuard no_autocast(c10::DispatchKey::AutocastCUDA);
+  const auto t = at::autocast::promote_type(at::kFloat, c10::DeviceType::CUDA, a, b, c, z);
+  static auto op = c10::Dispatcher::singleton()
+                       .findSchemaOrThrow("torchscience::hypergeometric_2_f_1", "")
+                       .typed<at::Tensor(const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                         const at::Tensor&)>();
+  const auto dev = c10::DeviceType::CUDA;
+  return op.call(at::autocast::cached_cast(t, a, dev), at::autocast::cached_cast(t, b, dev),
+                 at::autocast::cached_cast(t, c, dev), at::autocast::cached_cast(t, z, dev));
+}
+}  // namespace tsbh::ops
+
+TORCH_LIBRARY_IMPL(torchscience, CUDA, m) {
+  m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_cuda);
+  m.impl("hypergeometric_2_f_1_backward", tsbh::ops::hyp2f1_backward_cuda);
+  m.impl("hypergeometric_2_f_1_backward_backward", tsbh::ops::hyp2f1_backward_backward_cuda);
+}
+TORCH_LIBRARY_IMPL(torchscience, Meta, m) {
+  m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_meta);
+  m.impl("hypergeometric_2_f_1_backward", tsbh::ops::hyp2f1_backward_meta);
+  m.impl("hypergeometric_2_f_1_backward_backward", tsbh::ops::hyp2f1_backward_backward_meta);
+}
+TORCH_LIBRARY_IMPL(torchscience, CPU, m) {
+  m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_cpu);
+  m.impl("hypergeometric_2_f_1_backward", tsbh::ops::hyp2f1_backward_cpu);
+  m.impl("hypergeometric_2_f_1_backward_backward", tsbh::ops::hyp2f1_backward_backward_cpu);
+}
+TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_autograd); }
+TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_autocast); }
+
 // Library-level controls (not part of the reference's namespace).
 namespace tsbh {
 int64_t set_precision_mode(int64_t mode) {

@@ -118,10 +118,28 @@ def complete_legendre_elliptic_integral_e(m: Tensor) -> Tensor:
     return torch.ops.torchscience.complete_legendre_elliptic_integral_e(m)
 
 
+def hypergeometric_2_f_1(a: Tensor, b: Tensor, c: Tensor, z: Tensor) -> Tensor:
+    """Gauss hypergeometric function 2F1(a, b; c; z) for real arguments; NaN for z > 1.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_hypergeometric_2_f_1.py),
+    including its special values (hypergeometric_2_f_1.h:203-295). Every dtype is evaluated in FP64.
+    """
+    return torch.ops.torchscience.hypergeometric_2_f_1(a, b, c, z)
+
+
 __all__ = [
     "bessel_j",
     "bessel_j_0",
     "bessel_y",
+    "complete_legendre_elliptic_integral_e",
+    "complete_legendre_elliptic_integral_k",
+    "digamma",
+    "gamma",
+    "hypergeometric_2_f_1",
+    "log_gamma",
     "modified_bessel_i",
     "modified_bessel_k",
-   "complete_legendre_elliptic_integral_e", "complete_legendre_elliptic_integral_k", "digamma", "gamma", "log_gamma", "regularized_gamma_p", "regularized_gamma_q", "trigamma"]
+    "regularized_gamma_p",
+    "regularized_gamma_q",
+    "trigamma",
+]
