@@ -151,18 +151,14 @@ def timed_steps(fn, steps, warmup, flush):
 
 
 def count_launches(fn) -> int:
-    """Kernels of this library (names in namespace tsb::) launched by one step,
-    counted with the torch profiler (-1 if the profiler is unavailable, e.g.
-    under an external profiler)."""
-    try:
-        from torch.profiler import ProfilerActivity, profile
+    """Kernels this library launches in one call of fn, read from the
+    library's own launch counter (tsb_launch_count)."""
+    from torchscience_b200._cabi import lib
 
-        with profile(activities=[ProfilerActivity.CUDA]) as prof:
-            fn()
-            torch.cuda.synchronize()
-        return sum(1 for ev in prof.events() if ev.device_type == torch.autograd.DeviceType.CUDA and "tsb" in ev.name)
-    except Exception:
-        return -1
+    n0 = lib().tsb_launch_count()
+    fn()
+    torch.cuda.synchronize()
+    return int(lib().tsb_launch_count() - n0)
 
 
 def kernel_roofline(dev_inputs, steps, flush):

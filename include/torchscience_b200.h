@@ -84,6 +84,11 @@ const char* tsb_status_string(int32_t status);
  * them (cpu/macros.h:987-1032). */
 int64_t tsb_workspace_bytes(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_t n_out);
 
+/* Number of CUDA kernels this library has launched in this process, over all
+ * devices and threads (a diagnostic for counting launches; no counterpart in
+ * the reference, whose operators run on the CPU). */
+int64_t tsb_launch_count(void);
+
 /* Every op entry point has this signature. */
 #define TSB_OP_SIGNATURE(name)                                               \
   int32_t name(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out,    \

@@ -101,3 +101,19 @@ def test_valid_call_without_a_device_reports_device_error():
     L = lib()
     st = L.tsb_log_gamma(arr(desc([8])), 1, arr(desc([8])), 1, 0, None, ctypes.c_int64(0), None)
     assert st == -6
+
+
+def test_launch_counter_is_exported_and_starts_without_launches():
+    n = lib().tsb_launch_count()
+    assert n >= 0
+    # An empty iteration launches nothing.
+    from tests._util import TsbTensor
+
+    t = TsbTensor()
+    t.data, t.dtype, t.ndim = None, 1, 1
+    t.sizes[0] = 0
+    o = TsbTensor()
+    o.data, o.dtype, o.ndim = None, 1, 1
+    o.sizes[0] = 0
+    lib().tsb_log_gamma((TsbTensor * 1)(t), 1, (TsbTensor * 1)(o), 1, 0, None, 0, None)
+    assert lib().tsb_launch_count() == n

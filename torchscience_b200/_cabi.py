@@ -42,6 +42,7 @@ def lib():
         _lib.tsb_status_string.restype = ctypes.c_char_p
         _lib.tsb_version.restype = ctypes.c_char_p
         _lib.tsb_workspace_bytes.restype = ctypes.c_int64
+        _lib.tsb_launch_count.restype = ctypes.c_int64
     return _lib
 
 

@@ -2,6 +2,7 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -11,10 +12,13 @@ namespace tsb {
 
 namespace {
 thread_local std::string g_last_error;
+std::atomic<int64_t> g_launches{0};
 std::mutex g_dev_mutex;
 DeviceInfo g_devices[64];
 bool g_dev_init[64];
 }  // namespace
+
+void count_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int32_t set_error(int32_t status, const char* fmt, ...) {
   char buf[512];
@@ -62,6 +66,8 @@ int32_t current_device(int* dev, const DeviceInfo** info) {
 extern "C" {
 
 const char* tsb_version(void) { return "torchscience_b200 0.1.0 (sm_100a)"; }
+
+int64_t tsb_launch_count(void) { return tsb::g_launches.load(std::memory_order_relaxed); }
 
 const char* tsb_last_error(void) { return tsb::g_last_error.c_str(); }
 

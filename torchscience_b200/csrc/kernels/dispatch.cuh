@@ -15,6 +15,8 @@ namespace tsb {
 
 // Sets the calling thread's error message; returns `status`.
 int32_t set_error(int32_t status, const char* fmt, ...);
+// Adds n to the process-wide count of launched kernels (tsb_launch_count).
+void count_launches(int64_t n);
 
 struct DeviceInfo {
   int sm_count;
@@ -184,6 +186,7 @@ int32_t launch_map(const MapParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t stream, i
   const int64_t ntiles = (p.numel + S::TILE - 1) / S::TILE;
   const int64_t grid = std::min<int64_t>(ntiles, (int64_t)info->sm_count * occ);
   map_kernel<Fn, TS><<<(unsigned)grid, kBlock, smem, stream>>>(p);
+  count_launches(1);
   return check_launch("map kernel launch");
 }
 
@@ -195,6 +198,7 @@ int32_t launch_reduce(const Reduce2DParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t s
   const int64_t ntiles = p.n_row_tiles * p.n_col_tiles;
   const int64_t grid = std::min<int64_t>(ntiles, (int64_t)info->sm_count * occ);
   reduce2d_kernel<Fn, TS><<<(unsigned)grid, kBlock, smem, stream>>>(p);
+  count_launches(1);
   int32_t st = check_launch("reduce kernel launch");
   if (st) return st;
   for (int o = 0; o < Fn::NOUT; ++o) {
@@ -209,6 +213,8 @@ int32_t launch_reduce(const Reduce2DParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t s
     } else if (kind == kOutAll) {
       finalize_all_kernel<TS><<<1, kBlock, 0, stream>>>(p.ws[o], ntiles, p.out_ptr[o]);
     }
+    if (kind != kOutRow && kind != kOutCol && kind != kOutAll) continue;
+    count_launches(1);
     st = check_launch("finalize kernel launch");
     if (st) return st;
   }
@@ -317,6 +323,28 @@ int32_t run_op(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_
     if ((mask & (1u << o)) && output_is_reduced(c, NIN + o)) reduced = true;
   cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
   const bool use64 = precision == TSB_PRECISION_FP64;
+  if constexpr (HasAux<FD>::value) {
+    // A 2-D grid on which an input with per-row/column tables is broadcast
+    // runs through the tiled 2-D kernel (every output full), which builds the
+    // tables once per tile row / column.
+    if (!reduced && c.ndim == 2) {
+      const int ka = FD::AUX_IN0, kb = FD::AUX_IN1;
+      const bool bcast = c.stride[ka][0] == 0 || c.stride[ka][1] == 0 || c.stride[kb][0] == 0 || c.stride[kb][1] == 0;
+      if (bcast) {
+        Reduce2DParams<NIN, NOUT> p;
+        st = fill_reduce_params(c, in, out, mask, nullptr, 0, p);
+        if (st) return st;
+        switch (dtype) {
+          case TSB_F64: return launch_reduce<FD, double>(p, s, dev, info);
+          case TSB_F32:
+            return use64 ? launch_reduce<FD, float>(p, s, dev, info) : launch_reduce<FF, float>(p, s, dev, info);
+          case TSB_F16: return launch_reduce<FF, __half>(p, s, dev, info);
+          case TSB_BF16: return launch_reduce<FF, __nv_bfloat16>(p, s, dev, info);
+        }
+        return set_error(TSB_ERR_DTYPE, "unsupported dtype");
+      }
+    }
+  }
   if (!reduced) {
     MapParams<NIN, NOUT> p;
     fill_map_params(c, in, out, mask, p);

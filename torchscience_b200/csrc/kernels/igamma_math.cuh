@@ -60,20 +60,74 @@ __device__ inline double stirling_mu_d(double a) {
   return r * (1.0 / 12 - z * (1.0 / 360 - z * (1.0 / 1260 - z * (1.0 / 1680 - z * (1.0 / 1188 - z * (691.0 / 360360 - z * (1.0 / 156)))))));
 }
 
+// Quantities of a alone and of x alone.  On a broadcast grid they are
+// computed once per row / column (one value of a or x) into a table; an
+// element then reads them instead of recomputing lnΓ, ψ and the logarithms.
+// IgPre reads a table when it has one and computes the quantity otherwise,
+// with the same expression, so both give identical results.
+enum IgammaAuxA : int {
+  kIgA_LG = 0,  // a < 10: lnΓ(a+1); a >= 10: ½ln(2πa) + μ(a)
+  kIgA_LA,      // ln a
+  kIgA_RA,      // 1/a
+  kIgA_PSI,     // ψ(a)  (first and second derivatives)
+  kIgA_PSI1,    // ψ'(a) (second derivatives)
+  kIgA_LGF,     // lgammaf(a+1) in float (classification)
+  kIgA_LAF,     // __logf(a)
+  kIgA_LA1F,    // __logf(a+1)
+  kIgAuxA
+};
+enum IgammaAuxX : int {
+  kIgX_LX = 0,  // ln x
+  kIgX_LXF,     // __logf(x)
+  kIgAuxX
+};
+
+__device__ inline double igamma_lg(double a) {
+  return a < 10.0 ? lgamma(a + 1.0) : 0.5 * log(2.0 * CUDART_PI * a) + stirling_mu_d(a);
+}
+
+template <int ORDER>
+__device__ inline void igamma_aux_a(double a, double* o) {
+  const float af = (float)a;
+  o[kIgA_LG] = igamma_lg(a);
+  o[kIgA_LA] = log(a);
+  o[kIgA_RA] = 1.0 / a;
+  o[kIgA_PSI] = ORDER >= 1 ? digamma_d(a) : 0.0;
+  o[kIgA_PSI1] = ORDER >= 2 ? trigamma_d(a) : 0.0;
+  o[kIgA_LGF] = lgammaf(af + 1.0f);
+  o[kIgA_LAF] = __logf(af);
+  o[kIgA_LA1F] = __logf(af + 1.0f);
+}
+__device__ inline void igamma_aux_x(double x, double* o) {
+  o[kIgX_LX] = log(x);
+  o[kIgX_LXF] = __logf((float)x);
+}
+
+struct IgPre {
+  const double* A;  // table row for this a, or nullptr
+  const double* X;  // table entry for this x, or nullptr
+  double a, x;
+  __device__ double lg() const { return A ? A[kIgA_LG] : igamma_lg(a); }
+  __device__ double la() const { return A ? A[kIgA_LA] : log(a); }
+  __device__ double ra() const { return A ? A[kIgA_RA] : 1.0 / a; }
+  __device__ double psi() const { return A ? A[kIgA_PSI] : digamma_d(a); }
+  __device__ double psi1() const { return A ? A[kIgA_PSI1] : trigamma_d(a); }
+  __device__ float lgf() const { return A ? (float)A[kIgA_LGF] : lgammaf((float)a + 1.0f); }
+  __device__ float laf() const { return A ? (float)A[kIgA_LAF] : __logf((float)a); }
+  __device__ float la1f() const { return A ? (float)A[kIgA_LA1F] : __logf((float)a + 1.0f); }
+  __device__ double lx() const { return X ? X[kIgX_LX] : log(x); }
+  __device__ float lxf() const { return X ? (float)X[kIgX_LXF] : __logf((float)x); }
+};
+
 // ln D(a,x), D = x^a e^{-x} / Γ(a+1).
 // For a >= 10 the Temme form a·log1pmx(t) is used near x ~ a (|t| < 1/2);
 // farther out log(x/a) is formed directly so that 1 + t = x/a does not lose
 // the digits that t = (x-a)/a rounds away when x << a.
-__device__ inline double igamma_log_prefix_d(double a, double x) {
-  if (a < 10.0) return a * log(x) - x - lgamma(a + 1.0);
+__device__ inline double igamma_log_prefix_d(double a, double x, const IgPre& P) {
+  if (a < 10.0) return a * P.lx() - x - P.lg();
   const double t = (x - a) / a;
   const double core = fabs(t) < 0.5 ? a * log1pmx_d(t) : a * log(x / a) - (x - a);
-  return core - 0.5 * log(2.0 * CUDART_PI * a) - stirling_mu_d(a);
-}
-
-// Cheap float estimate of ln D used only to classify elements.
-__device__ __forceinline__ float igamma_log_prefix_est(float a, float x) {
-  return a * __logf(x) - x - lgammaf(a + 1.0f);
+  return core - P.lg();
 }
 
 // Series S = Σ_{n>=0} x^n / ((a+1)...(a+n)) and its a-derivatives.
@@ -239,11 +293,12 @@ __device__ __forceinline__ bool igamma_fp32_ok(int region) {
 }
 
 // Region of (a, x) from cheap float arithmetic.
-__device__ __forceinline__ int igamma_classify(double ad, double xd) {
+__device__ __forceinline__ int igamma_classify(double ad, double xd, const IgPre& P) {
   if (!(xd >= 0.0) || !(ad > 0.0) || xd == 0.0 || isinf(xd) || isinf(ad)) return kIgSpecial;
   const float a = (float)ad, x = (float)xd;
   if (!(a > 0.0f) || !(x > 0.0f) || isinf(a) || isinf(x)) return kIgSpecial;
-  const float lnd = igamma_log_prefix_est(a, x);
+  // float estimate of ln D
+  const float lnd = a * P.lxf() - x - P.lgf();
   // Saturation: the prefactor (and ∂P/∂x = D·a/x, whose ratio a/x is
   // included) is below e^-760, so in double P or Q and all derivatives are 0.
   // The float estimate is good to far better than the 15-unit margin to the
@@ -252,22 +307,25 @@ __device__ __forceinline__ int igamma_classify(double ad, double xd) {
   const float lam = x / (a + 1.0f);
   if (x < a + 1.0f) {
     // P <= D·(a+1)/(a+1-x) ~ D·a.
-    if (lnd + __logf(a + 1.0f) + lratio < -760.0f) return kIgSat0;
+    if (lnd + P.la1f() + lratio < -760.0f) return kIgSat0;
     if (a < 1.0f) return kIgSmallA;
     return lam < 0.1f ? kIgS0 : lam < 0.35f ? kIgS1 : lam < 0.7f ? kIgS2 : kIgS3;
   }
   // Q = a D F with F <= 1/(x+1-a) <= 1.
-  if (lnd + __logf(a) + lratio < -760.0f) return kIgSat1;
+  if (lnd + P.laf() + lratio < -760.0f) return kIgSat1;
   return lam > 3.0f ? kIgC0 : lam > 1.5f ? kIgC1 : kIgC2;
+}
+__device__ __forceinline__ int igamma_classify(double ad, double xd) {
+  return igamma_classify(ad, xd, IgPre{nullptr, nullptr, ad, xd});
 }
 
 // Q(a, x) for a < 1, x < a + 1 without the 1 - P cancellation (P -> 1 as
 // a -> 0): from γ(a,x) = Σ (-1)^n x^(a+n) / (n!(a+n)),
 //   Q = -expm1(a ln x - lnΓ(1+a)) - x^a/Γ(1+a) · a · Σ_{n>=1} (-x)^n / (n!(a+n)),
 // with lnΓ(1+a) = a·G(2a-1) from the fit in fits.cuh (no rounding of 1 + a).
-__device__ inline double igamma_q_small_a_d(double a, double x) {
+__device__ inline double igamma_q_small_a_d(double a, double x, double lx) {
   const double lg1p = a * horner(fits::LGAMMA1P_D, fma(2.0, a, -1.0));
-  const double e = a * log(x) - lg1p;
+  const double e = a * lx - lg1p;
   double term = 1.0, T = 0.0;
   for (int n = 1; n < 80; ++n) {
     term *= -x / (double)n;
@@ -281,7 +339,7 @@ __device__ inline double igamma_q_small_a_d(double a, double x) {
 // FP64 evaluation.  ORDER 0: p,q; 1: + pa, px; 2: + paa, pax, pxx.
 // WANT_Q: Q is requested (selects the small-a formula for Q where it matters).
 template <int ORDER, bool WANT_Q = false>
-__device__ inline IgammaOut igamma_eval_d(double a, double x) {
+__device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
   if (isnan(a) || isnan(x) || x < 0.0 || a <= 0.0) {
@@ -304,42 +362,46 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x) {
     o.q = 1.0;
     return o;
   }
-  const double lnD = igamma_log_prefix_d(a, x);
+  const double lnD = igamma_log_prefix_d(a, x, P);
+  const double lx = P.lx();
   // ∂P/∂x = x^(a-1) e^{-x} / Γ(a) = D·a/x
-  const double lnPx = lnD + log(a / x);
-  double psi_a = 0.0, psi1_a = 0.0;
-  if (ORDER >= 1) psi_a = digamma_d(a);
-  if (ORDER >= 2) psi1_a = trigamma_d(a);
-  const double lx = log(x);
+  const double lnPx = lnD + (P.la() - lx);
   if (x < a + 1.0) {
-    if (lnD + log(a + 1.0) < -760.0) {
+    if (lnD + log1p(a) < -760.0) {
       o.p = 0.0;
       o.q = 1.0;
       return o;
     }
+    double psi_a = 0.0, psi1_a = 0.0;
+    if (ORDER >= 1) psi_a = P.psi();
+    if (ORDER >= 2) psi1_a = P.psi1();
     double S, S1 = 0.0, S2 = 0.0;
     igamma_series<double, ORDER>(a, x, S, S1, S2);
     const double D = exp(lnD);
     o.p = D * S;
-    o.q = (WANT_Q && a < 1.0) ? igamma_q_small_a_d(a, x) : 1.0 - o.p;
+    o.q = (WANT_Q && a < 1.0) ? igamma_q_small_a_d(a, x, lx) : 1.0 - o.p;
     if (ORDER >= 1) {
-      const double L1 = lx - (psi_a + 1.0 / a);  // d lnD/da = ln x - ψ(a+1)
+      const double ra = P.ra();
+      const double L1 = lx - (psi_a + ra);  // d lnD/da = ln x - ψ(a+1)
       o.pa = D * fma(L1, S, S1);
       o.px = exp(lnPx);
       if (ORDER >= 2) {
-        const double L2 = -(psi1_a - 1.0 / (a * a));  // -ψ'(a+1)
+        const double L2 = -(psi1_a - ra * ra);  // -ψ'(a+1)
         o.paa = D * ((L2 + L1 * L1) * S + 2.0 * L1 * S1 + S2);
         o.pax = o.px * (lx - psi_a);
         o.pxx = o.px * ((a - 1.0) / x - 1.0);
       }
     }
   } else {
-    const double lnE = lnD + log(a);  // E = x^a e^{-x}/Γ(a)
+    const double lnE = lnD + P.la();  // E = x^a e^{-x}/Γ(a)
     if (lnE < -760.0) {
       o.p = 1.0;
       o.q = 0.0;
       return o;
     }
+    double psi_a = 0.0, psi1_a = 0.0;
+    if (ORDER >= 1) psi_a = P.psi();
+    if (ORDER >= 2) psi1_a = P.psi1();
     double F, F1 = 0.0, F2 = 0.0;
     igamma_cf<double, ORDER>(a, x, F, F1, F2);
     const double E = exp(lnE);
@@ -367,21 +429,21 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x) {
 // (large a near the transition x ~ a, where the term count grows like √a and
 // float accumulation would exceed 1e-6).
 template <int ORDER, bool WANT_Q = false>
-__device__ inline IgammaOut igamma_eval_m(int region, float af, float xf) {
+__device__ inline IgammaOut igamma_eval_m(int region, float af, float xf, const IgPre& P) {
   if (region == kIgSmallA) {
-    if (WANT_Q) return igamma_eval_d<ORDER, true>((double)af, (double)xf);
+    if (WANT_Q) return igamma_eval_d<ORDER, true>((double)af, (double)xf, P);
     region = kIgS1;
   }
-  if (!igamma_fp32_ok(region)) return igamma_eval_d<ORDER>((double)af, (double)xf);
+  if (!igamma_fp32_ok(region)) return igamma_eval_d<ORDER>((double)af, (double)xf, P);
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
   const double a = af, x = xf;
-  const double lnD = igamma_log_prefix_d(a, x);
-  const double lnPx = lnD + log(a / x);
+  const double lnD = igamma_log_prefix_d(a, x, P);
+  const double lx = P.lx();
+  const double lnPx = lnD + (P.la() - lx);
   double psi_a = 0.0, psi1_a = 0.0;
-  if (ORDER >= 1) psi_a = digamma_d(a);
-  if (ORDER >= 2) psi1_a = trigamma_d(a);
-  const double lx = log(x);
+  if (ORDER >= 1) psi_a = P.psi();
+  if (ORDER >= 2) psi1_a = P.psi1();
   if (region != kIgC0) {
     float Sf, S1f = 0.0f, S2f = 0.0f;
     igamma_series<float, ORDER>(af, xf, Sf, S1f, S2f);
@@ -390,11 +452,11 @@ __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf) {
     o.p = D * S;
     o.q = 1.0 - o.p;
     if (ORDER >= 1) {
-      const double L1 = lx - (psi_a + 1.0 / a);
+      const double L1 = lx - (psi_a + P.ra());
       o.pa = D * fma(L1, S, S1);
       o.px = exp(lnPx);
       if (ORDER >= 2) {
-        const double L2 = -(psi1_a - 1.0 / (a * a));
+        const double L2 = -(psi1_a - P.ra() * P.ra());
         o.paa = D * ((L2 + L1 * L1) * S + 2.0 * L1 * S1 + S2);
         o.pax = o.px * (lx - psi_a);
         o.pxx = o.px * ((a - 1.0) / x - 1.0);
@@ -404,7 +466,7 @@ __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf) {
     float Ff, F1f = 0.0f, F2f = 0.0f;
     igamma_cf<float, ORDER>(af, xf, Ff, F1f, F2f);
     const double F = Ff, F1 = F1f, F2 = F2f;
-    const double lnE = lnD + log(a);
+    const double lnE = lnD + P.la();
     const double E = exp(lnE);
     o.q = E * F;
     o.p = 1.0 - o.q;
@@ -432,14 +494,18 @@ __device__ __forceinline__ IgammaOut igamma_saturated(bool upper_is_zero) {
 }
 
 template <int ORDER, bool WANT_Q = false>
-__device__ __forceinline__ IgammaOut igamma_eval(int region, double a, double x) {
+__device__ __forceinline__ IgammaOut igamma_eval(int region, double a, double x, const IgPre& P) {
   if (region == kIgSat0 || region == kIgSat1) return igamma_saturated(region == kIgSat1);
-  return igamma_eval_d<ORDER, WANT_Q>(a, x);
+  return igamma_eval_d<ORDER, WANT_Q>(a, x, P);
 }
 template <int ORDER, bool WANT_Q = false>
-__device__ __forceinline__ IgammaOut igamma_eval(int region, float a, float x) {
+__device__ __forceinline__ IgammaOut igamma_eval(int region, float a, float x, const IgPre& P) {
   if (region == kIgSat0 || region == kIgSat1) return igamma_saturated(region == kIgSat1);
-  return igamma_eval_m<ORDER, WANT_Q>(region, a, x);
+  return igamma_eval_m<ORDER, WANT_Q>(region, a, x, P);
+}
+template <int ORDER, bool WANT_Q = false, typename T>
+__device__ __forceinline__ IgammaOut igamma_eval(int region, T a, T x) {
+  return igamma_eval<ORDER, WANT_Q>(region, a, x, IgPre{nullptr, nullptr, (double)a, (double)x});
 }
 
 }  // namespace tsb

@@ -11,54 +11,73 @@
 namespace tsb {
 
 // ∂P/∂x alone (backward with grad_a not requested): no series needed.
-__device__ __forceinline__ double igamma_px_only(double a, double x) {
+__device__ __forceinline__ double igamma_px_only(double a, double x, const IgPre& P) {
   if (isnan(a) || isnan(x) || x < 0.0 || a <= 0.0) return CUDART_NAN;
   if (x == 0.0 || isinf(x) || isinf(a)) return 0.0;
-  return exp(igamma_log_prefix_d(a, x) + log(a / x));
+  return exp(igamma_log_prefix_d(a, x, P) + (P.la() - P.lx()));
 }
 
+// Every functor here keeps per-row / per-column tables of its a and x inputs
+// (a quantities: lnΓ or the Stirling constant, ln a, 1/a, ψ(a), ψ'(a) and the
+// classifier's float values; x: ln x), which the 2-D kernel fills once per
+// tile row or column when the input is broadcast along the other dimension.
+template <int ORDER, int IA, int IX, typename T>
+struct IgammaAuxIO {
+  static constexpr int AUX_IN0 = IA, AUX_IN1 = IX;
+  static constexpr int NAUX0 = kIgAuxA, NAUX1 = kIgAuxX;
+  __device__ static void make_aux0(T v, double* o) { igamma_aux_a<ORDER>((double)v, o); }
+  __device__ static void make_aux1(T v, double* o) { igamma_aux_x((double)v, o); }
+  __device__ static IgPre pre(const T* in, const double* A, const double* X) {
+    return IgPre{A, X, (double)in[IA], (double)in[IX]};
+  }
+  __device__ static int classify(const T* in, const double* A = nullptr, const double* X = nullptr) {
+    return igamma_classify((double)in[IA], (double)in[IX], pre(in, A, X));
+  }
+};
+
 template <typename T_, bool UPPER>
-struct IgammaFwd {
+struct IgammaFwd : IgammaAuxIO<0, 0, 1, T_> {
   using T = T_;
   static constexpr int NIN = 2, NOUT = 1, R = kIgRegions;
   static constexpr bool REDUCE = false;
-  __device__ static int classify(const T* in) { return igamma_classify((double)in[0], (double)in[1]); }
-  __device__ static void eval(int r, const T* in, T* out, uint32_t) {
-    const IgammaOut o = igamma_eval<0, UPPER>(r, in[0], in[1]);
+  __device__ static void eval(int r, const T* in, T* out, uint32_t, const double* A = nullptr,
+                              const double* X = nullptr) {
+    const IgammaOut o = igamma_eval<0, UPPER>(r, in[0], in[1], IgammaFwd::pre(in, A, X));
     out[0] = (T)(UPPER ? o.q : o.p);
   }
 };
 
 template <typename T_, bool UPPER>
-struct IgammaBwd {
+struct IgammaBwd : IgammaAuxIO<1, 1, 2, T_> {
   using T = T_;
   static constexpr int NIN = 3, NOUT = 2, R = kIgRegions;
   static constexpr bool REDUCE = true;
-  __device__ static int classify(const T* in) { return igamma_classify((double)in[1], (double)in[2]); }
-  __device__ static void eval(int r, const T* in, T* out, uint32_t mask) {
+  __device__ static void eval(int r, const T* in, T* out, uint32_t mask, const double* A = nullptr,
+                              const double* X = nullptr) {
     const double sgn = UPPER ? -1.0 : 1.0;
     const double g = in[0];
+    const IgPre P = IgammaBwd::pre(in, A, X);
     if (!(mask & 1u)) {
       out[0] = T(0);
-      out[1] = (T)(sgn * g * igamma_px_only((double)in[1], (double)in[2]));
+      out[1] = (T)(sgn * g * igamma_px_only((double)in[1], (double)in[2], P));
       return;
     }
-    const IgammaOut o = igamma_eval<1>(r, in[1], in[2]);
+    const IgammaOut o = igamma_eval<1>(r, in[1], in[2], P);
     out[0] = (T)(sgn * g * o.pa);
     out[1] = (T)(sgn * g * o.px);
   }
 };
 
 template <typename T_, bool UPPER>
-struct IgammaBwdBwd {
+struct IgammaBwdBwd : IgammaAuxIO<2, 3, 4, T_> {
   using T = T_;
   static constexpr int NIN = 5, NOUT = 3, R = kIgRegions;
   static constexpr bool REDUCE = true;
-  __device__ static int classify(const T* in) { return igamma_classify((double)in[3], (double)in[4]); }
-  __device__ static void eval(int r, const T* in, T* out, uint32_t) {
+  __device__ static void eval(int r, const T* in, T* out, uint32_t, const double* A = nullptr,
+                              const double* X = nullptr) {
     const double sgn = UPPER ? -1.0 : 1.0;
     const double gga = in[0], ggx = in[1], g = in[2];
-    const IgammaOut o = igamma_eval<2>(r, in[3], in[4]);
+    const IgammaOut o = igamma_eval<2>(r, in[3], in[4], IgammaBwdBwd::pre(in, A, X));
     out[0] = (T)(sgn * (gga * o.pa + ggx * o.px));
     out[1] = (T)(sgn * g * (gga * o.paa + ggx * o.pax));
     out[2] = (T)(sgn * g * (gga * o.pax + ggx * o.pxx));

@@ -34,6 +34,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "torchscience_b200.h"
 
 namespace tsb {
@@ -202,6 +204,34 @@ __device__ __forceinline__ void carve(unsigned char* base, typename S::T*& buf, 
   regs = reinterpret_cast<uint8_t*>(list + S::TILE);
 }
 
+// Optional per-input tables (functors that define NAUX0): quantities of one
+// input alone (e.g. lnΓ(a), ψ(a), ln x) that a 2-D tile computes once per
+// row or column into shared memory when that input is constant along the
+// other dimension.  Such a functor provides
+//   AUX_IN0, AUX_IN1          the two inputs with tables,
+//   NAUX0, NAUX1              doubles per table entry,
+//   make_aux0(v, o), make_aux1(v, o),
+//   classify(in, aux0, aux1), eval(r, in, out, mask, aux0, aux1)
+// where a null table pointer means "compute the quantity here".
+template <class Fn, class = void>
+struct HasAux {
+  static constexpr bool value = false;
+  static constexpr int N0 = 1, N1 = 1;
+};
+template <class Fn>
+struct HasAux<Fn, decltype((void)Fn::NAUX0, void())> {
+  static constexpr bool value = true;
+  static constexpr int N0 = Fn::NAUX0, N1 = Fn::NAUX1;
+};
+
+// Table modes: 0 none (computed per element), 1 one entry per tile row,
+// 2 one entry per tile column.
+__device__ __forceinline__ int aux_mode(int64_t s0, int64_t s1) { return s1 == 0 ? 1 : (s0 == 0 ? 2 : 0); }
+template <int N>
+__device__ __forceinline__ const double* aux_at(const double* tab, int mode, int li) {
+  return mode == 1 ? tab + (li / 32) * N : (mode == 2 ? tab + (li % 32) * N : nullptr);
+}
+
 // Buckets the tile's local indices by region.  reg[k] is the region of
 // local index k*kBlock + tid, or R for an invalid slot.  On return
 // list[0..count) holds the valid local indices grouped by region and
@@ -259,6 +289,24 @@ __device__ __forceinline__ void cta_eval_sorted(int count, typename Fn::T* buf, 
 #pragma unroll
     for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * TILE + li];
     Fn::eval(regs[li], v, o, mask);
+#pragma unroll
+    for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
+  }
+  __syncthreads();
+}
+
+// cta_eval_sorted for functors with per-row / per-column tables (2-D tiles).
+template <class Fn, int TILE>
+__device__ __forceinline__ void cta_eval_sorted_aux(int count, typename Fn::T* buf, const uint16_t* list,
+                                                    const uint8_t* regs, uint32_t mask, const double* aux0, int mode0,
+                                                    const double* aux1, int mode1) {
+  using T = typename Fn::T;
+  for (int j = threadIdx.x; j < count; j += kBlock) {
+    const int li = list[j];
+    T v[Fn::NIN], o[Fn::NOUT];
+#pragma unroll
+    for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * TILE + li];
+    Fn::eval(regs[li], v, o, mask, aux_at<Fn::NAUX0>(aux0, mode0, li), aux_at<Fn::NAUX1>(aux1, mode1, li));
 #pragma unroll
     for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
   }
@@ -344,19 +392,41 @@ __global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<F
   constexpr int NIN = Fn::NIN, NOUT = Fn::NOUT, R = Fn::R;
   constexpr int EPT = S::EPT, TILE = S::TILE;
   constexpr int RR = R > 1 ? R : 1;
+  constexpr bool AUX = HasAux<Fn>::value;
+  constexpr int N0 = HasAux<Fn>::N0, N1 = HasAux<Fn>::N1;
   extern __shared__ __align__(16) unsigned char s_dyn[];
   __shared__ int s_cnt[RR], s_base[RR + 1];
   __shared__ double s_red[kBlock / 32][kTC];
+  __shared__ double s_aux0[AUX ? kTR * N0 : 1], s_aux1[AUX ? kTR * N1 : 1];
   T* buf;
   uint16_t* list;
   uint8_t* regs;
   carve<S>(s_dyn, buf, list, regs);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t ntiles = p.n_row_tiles * p.n_col_tiles;
+  int mode0 = 0, mode1 = 0;
+  if constexpr (AUX) {
+    mode0 = aux_mode(p.in_s0[Fn::AUX_IN0], p.in_s1[Fn::AUX_IN0]);
+    mode1 = aux_mode(p.in_s0[Fn::AUX_IN1], p.in_s1[Fn::AUX_IN1]);
+  }
 
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t rt = t / p.n_col_tiles, ct = t % p.n_col_tiles;
     const int64_t r0 = rt * kTR, c0 = ct * kTC;
+    if constexpr (AUX) {
+      // Tables for this tile: warp 0 fills input AUX_IN0's, warp 1 AUX_IN1's.
+      const int which = warp, mode = which == 0 ? mode0 : mode1;
+      if (which < 2 && mode != 0) {
+        const int64_t r = mode == 1 ? r0 + lane : r0, c = mode == 1 ? c0 : c0 + lane;
+        if (r < p.rows && c < p.cols) {
+          const int q = which == 0 ? Fn::AUX_IN0 : Fn::AUX_IN1;
+          const T v = load_as<TS, T>(p.in_ptr[q] + (r * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
+          if (which == 0) Fn::make_aux0(v, s_aux0 + lane * N0);
+          else Fn::make_aux1(v, s_aux1 + lane * N1);
+        }
+      }
+      __syncthreads();
+    }
     int reg[EPT];
 #pragma unroll
     for (int k = 0; k < EPT; ++k) {
@@ -368,13 +438,17 @@ __global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<F
 #pragma unroll
         for (int q = 0; q < NIN; ++q)
           v[q] = load_as<TS, T>(p.in_ptr[q] + (r * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
-        if constexpr (R > 1) reg[k] = Fn::classify(v);
+        if constexpr (AUX) reg[k] = Fn::classify(v, aux_at<N0>(s_aux0, mode0, li), aux_at<N1>(s_aux1, mode1, li));
+        else if constexpr (R > 1) reg[k] = Fn::classify(v);
         else reg[k] = 0;
 #pragma unroll
         for (int q = 0; q < NIN; ++q) buf[q * TILE + li] = v[q];
       }
     }
-    if constexpr (R > 1) {
+    if constexpr (AUX) {
+      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base);
+      cta_eval_sorted_aux<Fn, TILE>(count, buf, list, regs, p.out_mask, s_aux0, mode0, s_aux1, mode1);
+    } else if constexpr (R > 1) {
       const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base);
       cta_eval_sorted<Fn, TILE>(count, buf, list, regs, p.out_mask);
     } else {
