@@ -95,7 +95,7 @@ int64_t tsb_workspace_bytes(const tsb_tensor* in, int32_t n_in, const tsb_tensor
   if (!reduced) return 0;
   if (c.ndim > 2)
     return tsb::set_error(TSB_ERR_LAYOUT, "reduced outputs need an iteration space of at most 2 coalesced dims");
-  return tsb::reduce_ws_bytes(c, n_in, out, n_out, tsb::kTR);
+  return tsb::reduce_ws_bytes(c, n_in, out, n_out, tsb::kTRMin);
 }
 
 }  // extern "C"

@@ -190,9 +190,16 @@ int32_t launch_map(const MapParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t stream, i
   return check_launch("map kernel launch");
 }
 
+template <int NIN, int NOUT>
+inline int32_t fill_reduce_params(const Canon& c, const tsb_tensor* in, const tsb_tensor* out, uint32_t mask, void* ws,
+                                  int64_t ws_bytes, int tr, Reduce2DParams<NIN, NOUT>& p);
+
 template <class Fn, typename TS>
-int32_t launch_reduce(const Reduce2DParams<Fn::NIN, Fn::NOUT>& p, cudaStream_t stream, int dev,
-                      const DeviceInfo* info) {
+int32_t launch_reduce(const Canon& c, const tsb_tensor* in, const tsb_tensor* out, uint32_t mask, void* ws,
+                      int64_t ws_bytes, cudaStream_t stream, int dev, const DeviceInfo* info) {
+  Reduce2DParams<Fn::NIN, Fn::NOUT> p;
+  const int32_t fst = fill_reduce_params(c, in, out, mask, ws, ws_bytes, ReduceTile<Fn>::TR, p);
+  if (fst) return fst;
   constexpr size_t smem = ReduceStage<Fn>::SMEM;
   const int occ = occupancy_for<ReduceTag<Fn, TS>>(reduce2d_kernel<Fn, TS>, kBlock, smem, dev);
   const int64_t ntiles = p.n_row_tiles * p.n_col_tiles;
@@ -241,8 +248,8 @@ inline void fill_map_params(const Canon& c, const tsb_tensor* in, const tsb_tens
 
 template <int NIN, int NOUT>
 inline int32_t fill_reduce_params(const Canon& c, const tsb_tensor* in, const tsb_tensor* out, uint32_t mask,
-                                  void* ws, int64_t ws_bytes, Reduce2DParams<NIN, NOUT>& p) {
-  constexpr int TR = kTR;
+                                  void* ws, int64_t ws_bytes, int tr, Reduce2DParams<NIN, NOUT>& p) {
+  const int TR = tr;
   if (c.ndim > 2)
     return set_error(TSB_ERR_LAYOUT,
                      "reduced outputs need an iteration space that coalesces to at most 2 dims (got %d)", c.ndim);
@@ -331,15 +338,13 @@ int32_t run_op(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_
       const int ka = FD::AUX_IN0, kb = FD::AUX_IN1;
       const bool bcast = c.stride[ka][0] == 0 || c.stride[ka][1] == 0 || c.stride[kb][0] == 0 || c.stride[kb][1] == 0;
       if (bcast) {
-        Reduce2DParams<NIN, NOUT> p;
-        st = fill_reduce_params(c, in, out, mask, nullptr, 0, p);
-        if (st) return st;
         switch (dtype) {
-          case TSB_F64: return launch_reduce<FD, double>(p, s, dev, info);
+          case TSB_F64: return launch_reduce<FD, double>(c, in, out, mask, nullptr, 0, s, dev, info);
           case TSB_F32:
-            return use64 ? launch_reduce<FD, float>(p, s, dev, info) : launch_reduce<FF, float>(p, s, dev, info);
-          case TSB_F16: return launch_reduce<FF, __half>(p, s, dev, info);
-          case TSB_BF16: return launch_reduce<FF, __nv_bfloat16>(p, s, dev, info);
+            return use64 ? launch_reduce<FD, float>(c, in, out, mask, nullptr, 0, s, dev, info)
+                         : launch_reduce<FF, float>(c, in, out, mask, nullptr, 0, s, dev, info);
+          case TSB_F16: return launch_reduce<FF, __half>(c, in, out, mask, nullptr, 0, s, dev, info);
+          case TSB_BF16: return launch_reduce<FF, __nv_bfloat16>(c, in, out, mask, nullptr, 0, s, dev, info);
         }
         return set_error(TSB_ERR_DTYPE, "unsupported dtype");
       }
@@ -357,14 +362,13 @@ int32_t run_op(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_
     return set_error(TSB_ERR_DTYPE, "unsupported dtype");
   }
   if constexpr (FD::REDUCE) {
-    Reduce2DParams<NIN, NOUT> p;
-    st = fill_reduce_params(c, in, out, mask, ws, ws_bytes, p);
-    if (st) return st;
     switch (dtype) {
-      case TSB_F64: return launch_reduce<FD, double>(p, s, dev, info);
-      case TSB_F32: return use64 ? launch_reduce<FD, float>(p, s, dev, info) : launch_reduce<FF, float>(p, s, dev, info);
-      case TSB_F16: return launch_reduce<FF, __half>(p, s, dev, info);
-      case TSB_BF16: return launch_reduce<FF, __nv_bfloat16>(p, s, dev, info);
+      case TSB_F64: return launch_reduce<FD, double>(c, in, out, mask, ws, ws_bytes, s, dev, info);
+      case TSB_F32:
+        return use64 ? launch_reduce<FD, float>(c, in, out, mask, ws, ws_bytes, s, dev, info)
+                     : launch_reduce<FF, float>(c, in, out, mask, ws, ws_bytes, s, dev, info);
+      case TSB_F16: return launch_reduce<FF, __half>(c, in, out, mask, ws, ws_bytes, s, dev, info);
+      case TSB_BF16: return launch_reduce<FF, __nv_bfloat16>(c, in, out, mask, ws, ws_bytes, s, dev, info);
     }
     return set_error(TSB_ERR_DTYPE, "unsupported dtype");
   } else {

@@ -78,6 +78,7 @@ enum IgammaAuxA : int {
 };
 enum IgammaAuxX : int {
   kIgX_LX = 0,  // ln x
+  kIgX_RX,      // 1/x
   kIgX_LXF,     // __logf(x)
   kIgAuxX
 };
@@ -100,6 +101,7 @@ __device__ inline void igamma_aux_a(double a, double* o) {
 }
 __device__ inline void igamma_aux_x(double x, double* o) {
   o[kIgX_LX] = log(x);
+  o[kIgX_RX] = 1.0 / x;
   o[kIgX_LXF] = __logf((float)x);
 }
 
@@ -116,6 +118,7 @@ struct IgPre {
   __device__ float laf() const { return A ? (float)A[kIgA_LAF] : __logf((float)a); }
   __device__ float la1f() const { return A ? (float)A[kIgA_LA1F] : __logf((float)a + 1.0f); }
   __device__ double lx() const { return X ? X[kIgX_LX] : log(x); }
+  __device__ double rx() const { return X ? X[kIgX_RX] : 1.0 / x; }
   __device__ float lxf() const { return X ? (float)X[kIgX_LXF] : __logf((float)x); }
 };
 
@@ -128,6 +131,12 @@ __device__ inline double igamma_log_prefix_d(double a, double x, const IgPre& P)
   const double t = (x - a) / a;
   const double core = fabs(t) < 0.5 ? a * log1pmx_d(t) : a * log(x / a) - (x - a);
   return core - P.lg();
+}
+
+// ∂P/∂x = D·a/x from D = exp(lnD), or from its logarithm where D itself
+// underflows (lnD < -700) but a/x lifts it back into range.
+__device__ __forceinline__ double igamma_px_from(double D, double lnD, double a, const IgPre& P) {
+  return lnD > -700.0 ? D * a * P.rx() : exp(lnD + (P.la() - P.lx()));
 }
 
 // Series S = Σ_{n>=0} x^n / ((a+1)...(a+n)) and its a-derivatives.
@@ -273,17 +282,19 @@ struct IgammaOut {
 // continued-fraction regions are split by the ratio that sets their
 // iteration count, so the lanes of a warp run loops of similar length.
 enum IgammaRegion : int {
-  kIgSpecial = 0,  // NaN / domain / x == 0 / x == inf
-  kIgS0 = 1,       // series, x/(a+1) < 0.1
-  kIgS1 = 2,       // series, x/(a+1) < 0.35
-  kIgS2 = 3,       // series, x/(a+1) < 0.7
-  kIgS3 = 4,       // series, x/(a+1) < 1
-  kIgC0 = 5,       // continued fraction, x/(a+1) > 3
-  kIgC1 = 6,       // continued fraction, x/(a+1) > 1.5
-  kIgC2 = 7,       // continued fraction, x/(a+1) <= 1.5
-  kIgSmallA = 8,   // a < 1, x < a + 1: series for P, dedicated formula for Q
-  kIgSat0 = 9,     // P and every derivative underflow to 0 (Q = 1)
-  kIgSat1 = 10,    // Q and every derivative underflow to 0 (P = 1)
+  // Numbered by decreasing cost (measured per element on B200), so that a
+  // tile's sorted list starts with its most expensive groups.
+  kIgS3 = 0,      // series, x/(a+1) < 1
+  kIgC2 = 1,      // continued fraction, x/(a+1) <= 1.5
+  kIgC1 = 2,      // continued fraction, x/(a+1) > 1.5
+  kIgS2 = 3,      // series, x/(a+1) < 0.7
+  kIgC0 = 4,      // continued fraction, x/(a+1) > 3
+  kIgS1 = 5,      // series, x/(a+1) < 0.35
+  kIgS0 = 6,      // series, x/(a+1) < 0.1
+  kIgSmallA = 7,  // a < 1, x < a + 1: series for P, dedicated formula for Q
+  kIgSat1 = 8,    // Q and every derivative underflow to 0 (P = 1)
+  kIgSat0 = 9,    // P and every derivative underflow to 0 (Q = 1)
+  kIgSpecial = 10,  // NaN / domain / x == 0 / x == inf
   kIgRegions = 11
 };
 
@@ -365,7 +376,6 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
   const double lnD = igamma_log_prefix_d(a, x, P);
   const double lx = P.lx();
   // ∂P/∂x = x^(a-1) e^{-x} / Γ(a) = D·a/x
-  const double lnPx = lnD + (P.la() - lx);
   if (x < a + 1.0) {
     if (lnD + log1p(a) < -760.0) {
       o.p = 0.0;
@@ -384,7 +394,7 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
       const double ra = P.ra();
       const double L1 = lx - (psi_a + ra);  // d lnD/da = ln x - ψ(a+1)
       o.pa = D * fma(L1, S, S1);
-      o.px = exp(lnPx);
+      o.px = igamma_px_from(D, lnD, a, P);
       if (ORDER >= 2) {
         const double L2 = -(psi1_a - ra * ra);  // -ψ'(a+1)
         o.paa = D * ((L2 + L1 * L1) * S + 2.0 * L1 * S1 + S2);
@@ -411,7 +421,7 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
       const double E1 = lx - psi_a;
       const double qa = E * fma(E1, F, F1);
       o.pa = -qa;
-      o.px = exp(lnPx);
+      o.px = lnE > -700.0 ? E * P.rx() : exp(lnE - lx);  // E/x
       if (ORDER >= 2) {
         const double E2 = -psi1_a;
         o.paa = -E * ((E2 + E1 * E1) * F + 2.0 * E1 * F1 + F2);
@@ -440,7 +450,6 @@ __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf, const 
   const double a = af, x = xf;
   const double lnD = igamma_log_prefix_d(a, x, P);
   const double lx = P.lx();
-  const double lnPx = lnD + (P.la() - lx);
   double psi_a = 0.0, psi1_a = 0.0;
   if (ORDER >= 1) psi_a = P.psi();
   if (ORDER >= 2) psi1_a = P.psi1();
@@ -454,7 +463,7 @@ __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf, const 
     if (ORDER >= 1) {
       const double L1 = lx - (psi_a + P.ra());
       o.pa = D * fma(L1, S, S1);
-      o.px = exp(lnPx);
+      o.px = igamma_px_from(D, lnD, a, P);
       if (ORDER >= 2) {
         const double L2 = -(psi1_a - P.ra() * P.ra());
         o.paa = D * ((L2 + L1 * L1) * S + 2.0 * L1 * S1 + S2);
@@ -473,7 +482,7 @@ __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf, const 
     if (ORDER >= 1) {
       const double E1 = lx - psi_a;
       o.pa = -E * fma(E1, F, F1);
-      o.px = exp(lnPx);
+      o.px = lnE > -700.0 ? E * P.rx() : exp(lnE - lx);  // E/x
       if (ORDER >= 2) {
         const double E2 = -psi1_a;
         o.paa = -E * ((E2 + E1 * E1) * F + 2.0 * E1 * F1 + F2);

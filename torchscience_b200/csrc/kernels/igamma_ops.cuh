@@ -8,6 +8,11 @@
 #include "dispatch.cuh"
 #include "igamma_math.cuh"
 
+#ifndef TSB_IGF_MINB
+#define TSB_IGF_MINB 4
+#endif
+
+
 namespace tsb {
 
 // ∂P/∂x alone (backward with grad_a not requested): no series needed.
@@ -39,6 +44,7 @@ template <typename T_, bool UPPER>
 struct IgammaFwd : IgammaAuxIO<0, 0, 1, T_> {
   using T = T_;
   static constexpr int NIN = 2, NOUT = 1, R = kIgRegions;
+  static constexpr int MIN_BLOCKS = TSB_IGF_MINB;
   static constexpr bool REDUCE = false;
   __device__ static void eval(int r, const T* in, T* out, uint32_t, const double* A = nullptr,
                               const double* X = nullptr) {
@@ -51,6 +57,9 @@ template <typename T_, bool UPPER>
 struct IgammaBwd : IgammaAuxIO<1, 1, 2, T_> {
   using T = T_;
   static constexpr int NIN = 3, NOUT = 2, R = kIgRegions;
+  // 64 registers, 4 resident CTAs: measured 15% faster than the unconstrained
+  // allocation (118 registers, 2 CTAs) on the 4096 x 4096 grid.
+  static constexpr int MIN_BLOCKS = 4;
   static constexpr bool REDUCE = true;
   __device__ static void eval(int r, const T* in, T* out, uint32_t mask, const double* A = nullptr,
                               const double* X = nullptr) {

@@ -176,14 +176,13 @@ __device__ __forceinline__ void store_element(const MapParams<Fn::NIN, Fn::NOUT>
 // ------------------------------------------------------------ CTA tiles
 // Map kernels stage tiles of up to 2048 elements (1024 when the operands
 // need more shared memory); the 2-D reduction uses 32 x 32 tiles.
-constexpr int kTC = 32;                 // 2-D tile columns (one per lane)
-constexpr int kTR = 32;                 // 2-D tile rows
-constexpr int kTile2D = kTC * kTR;      // 1024
+constexpr int kTC = 32;     // 2-D tile columns (one per lane)
+constexpr int kTRMin = 32;  // smallest 2-D tile height (sizes the generic workspace query)
 
-template <class Fn, int TILE_>
+template <class Fn, int TILE_, int NBUF_ = (Fn::NIN > Fn::NOUT ? Fn::NIN : Fn::NOUT)>
 struct Stage {
   using T = typename Fn::T;
-  static constexpr int NBUF = Fn::NIN > Fn::NOUT ? Fn::NIN : Fn::NOUT;
+  static constexpr int NBUF = NBUF_;
   static constexpr int TILE = TILE_;
   static constexpr int EPT = TILE / kBlock;
   // operand staging + region-sorted list (uint16) + region ids (uint8)
@@ -224,6 +223,26 @@ struct HasAux<Fn, decltype((void)Fn::NAUX0, void())> {
   static constexpr int N0 = Fn::NAUX0, N1 = Fn::NAUX1;
 };
 
+// Resident CTAs per SM the register allocation must allow (functors may set
+// MIN_BLOCKS; the default leaves registers unconstrained).
+template <class Fn, class = void>
+struct MinBlocks {
+  static constexpr int value = 1;
+};
+template <class Fn>
+struct MinBlocks<Fn, decltype((void)Fn::MIN_BLOCKS, void())> {
+  static constexpr int value = Fn::MIN_BLOCKS;
+};
+
+template <class Fn, class = void>
+struct HasAuxIdx {
+  static constexpr int i0 = -1, i1 = -1;
+};
+template <class Fn>
+struct HasAuxIdx<Fn, decltype((void)Fn::NAUX0, void())> {
+  static constexpr int i0 = Fn::AUX_IN0, i1 = Fn::AUX_IN1;
+};
+
 // Table modes: 0 none (computed per element), 1 one entry per tile row,
 // 2 one entry per tile column.
 __device__ __forceinline__ int aux_mode(int64_t s0, int64_t s1) { return s1 == 0 ? 1 : (s0 == 0 ? 2 : 0); }
@@ -239,7 +258,7 @@ __device__ __forceinline__ const double* aux_at(const double* tab, int mode, int
 // order; results do not, each element being evaluated independently.)
 template <int R, int EPT>
 __device__ __forceinline__ int cta_sort_by_region(const int (&reg)[EPT], uint16_t* list, uint8_t* regs, int* s_cnt,
-                                                  int* s_base) {
+                                                  int* s_base, int* s_next) {
   const int tid = threadIdx.x, lane = tid & 31;
   const unsigned lt = (1u << lane) - 1u;
   if (tid < R) s_cnt[tid] = 0;
@@ -259,6 +278,7 @@ __device__ __forceinline__ int cta_sort_by_region(const int (&reg)[EPT], uint16_
       acc += s_cnt[r];
     }
     s_base[R] = acc;
+    *s_next = 0;
   }
   __syncthreads();
   if (tid < R) s_cnt[tid] = s_base[tid];
@@ -276,45 +296,41 @@ __device__ __forceinline__ int cta_sort_by_region(const int (&reg)[EPT], uint16_
   return s_base[R];
 }
 
-// Evaluates the sorted tile in place.  Thread t takes sorted slots t,
-// t + kBlock, ...: warp w gets 32-slot groups w, w + 8, ..., a round-robin
-// spread of every region over the warps that keeps their loads balanced.
-template <class Fn, int TILE>
-__device__ __forceinline__ void cta_eval_sorted(int count, typename Fn::T* buf, const uint16_t* list,
-                                                const uint8_t* regs, uint32_t mask) {
+// Evaluates the sorted tile in place.  Warps take the 32-slot groups of the
+// sorted list dynamically from a shared counter, in list order: regions are
+// numbered by decreasing cost, so the expensive groups start first and the
+// tile's closing barrier waits on the cheapest ones.
+template <class Fn, int TILE, bool AUX>
+__device__ __forceinline__ void cta_eval_groups(int count, typename Fn::T* buf, const uint16_t* list,
+                                                const uint8_t* regs, uint32_t mask, int* s_next, const double* aux0,
+                                                int mode0, const double* aux1, int mode1) {
   using T = typename Fn::T;
-  for (int j = threadIdx.x; j < count; j += kBlock) {
-    const int li = list[j];
-    T v[Fn::NIN], o[Fn::NOUT];
+  const int lane = threadIdx.x & 31;
+  const int ngroups = (count + 31) >> 5;
+  for (;;) {
+    int gidx = 0;
+    if (lane == 0) gidx = atomicAdd(s_next, 1);
+    gidx = __shfl_sync(0xffffffffu, gidx, 0);
+    if (gidx >= ngroups) break;
+    const int j = (gidx << 5) + lane;
+    if (j < count) {
+      const int li = list[j];
+      T v[Fn::NIN], o[Fn::NOUT];
 #pragma unroll
-    for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * TILE + li];
-    Fn::eval(regs[li], v, o, mask);
+      for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * TILE + li];
+      if constexpr (AUX)
+        Fn::eval(regs[li], v, o, mask, aux_at<Fn::NAUX0>(aux0, mode0, li), aux_at<Fn::NAUX1>(aux1, mode1, li));
+      else
+        Fn::eval(regs[li], v, o, mask);
 #pragma unroll
-    for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
-  }
-  __syncthreads();
-}
-
-// cta_eval_sorted for functors with per-row / per-column tables (2-D tiles).
-template <class Fn, int TILE>
-__device__ __forceinline__ void cta_eval_sorted_aux(int count, typename Fn::T* buf, const uint16_t* list,
-                                                    const uint8_t* regs, uint32_t mask, const double* aux0, int mode0,
-                                                    const double* aux1, int mode1) {
-  using T = typename Fn::T;
-  for (int j = threadIdx.x; j < count; j += kBlock) {
-    const int li = list[j];
-    T v[Fn::NIN], o[Fn::NOUT];
-#pragma unroll
-    for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * TILE + li];
-    Fn::eval(regs[li], v, o, mask, aux_at<Fn::NAUX0>(aux0, mode0, li), aux_at<Fn::NAUX1>(aux1, mode1, li));
-#pragma unroll
-    for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
+      for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
+    }
   }
   __syncthreads();
 }
 
 template <class Fn, typename TS>
-__global__ void __launch_bounds__(kBlock) map_kernel(const MapParams<Fn::NIN, Fn::NOUT> p) {
+__global__ void __launch_bounds__(kBlock, MinBlocks<Fn>::value) map_kernel(const MapParams<Fn::NIN, Fn::NOUT> p) {
   using T = typename Fn::T;
   using S = typename MapTile<Fn>::S;
   constexpr int NIN = Fn::NIN, NOUT = Fn::NOUT, R = Fn::R;
@@ -342,7 +358,7 @@ __global__ void __launch_bounds__(kBlock) map_kernel(const MapParams<Fn::NIN, Fn
     }
   } else {
     extern __shared__ __align__(16) unsigned char s_dyn[];
-    __shared__ int s_cnt[R], s_base[R + 1];
+    __shared__ int s_cnt[R], s_base[R + 1], s_next;
     T* buf;
     uint16_t* list;
     uint8_t* regs;
@@ -363,8 +379,8 @@ __global__ void __launch_bounds__(kBlock) map_kernel(const MapParams<Fn::NIN, Fn
           for (int q = 0; q < NIN; ++q) buf[q * TILE + li] = v[q];
         }
       }
-      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base);
-      cta_eval_sorted<Fn, TILE>(count, buf, list, regs, p.out_mask);
+      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base, &s_next);
+      cta_eval_groups<Fn, TILE, false>(count, buf, list, regs, p.out_mask, &s_next, nullptr, 0, nullptr, 0);
 #pragma unroll
       for (int k = 0; k < EPT; ++k) {
         const int li = k * kBlock + tid;
@@ -382,22 +398,50 @@ __global__ void __launch_bounds__(kBlock) map_kernel(const MapParams<Fn::NIN, Fn
 }
 
 // ------------------------------------------------------------ 2-D reduction
+// 2-D tiles are 64 x 32 (2048 elements) when the staging fits in 64 KB,
+// otherwise 32 x 32: more elements per tile spread each region's groups over
+// more warps and amortise the tile's barriers and table fills.
+// A functor with tables stages only its other inputs: the table inputs are
+// read from their tables (or, when an input varies along both dimensions,
+// again from global memory) at evaluation.
 template <class Fn>
-using ReduceStage = Stage<Fn, kTile2D>;
+struct ReduceTile {
+  static constexpr int NSTAGED = HasAux<Fn>::value ? Fn::NIN - 2 : Fn::NIN;
+  static constexpr int NBUF = NSTAGED > Fn::NOUT ? NSTAGED : Fn::NOUT;
+  static constexpr int TR = Stage<Fn, 64 * kTC, NBUF>::SMEM <= 64 * 1024 ? 64 : kTRMin;
+  using S = Stage<Fn, TR * kTC, NBUF>;
+  // staging slot of input q (-1: a table input)
+  __host__ __device__ static constexpr int slot(int q) {
+    if (!HasAux<Fn>::value) return q;
+    int k = 0;
+    for (int i = 0; i < q; ++i)
+      if (!is_table_input(i)) ++k;
+    return is_table_input(q) ? -1 : k;
+  }
+  __host__ __device__ static constexpr bool is_table_input(int q) {
+    if constexpr (HasAux<Fn>::value) return q == HasAuxIdx<Fn>::i0 || q == HasAuxIdx<Fn>::i1;
+    return false;
+  }
+};
+template <class Fn>
+using ReduceStage = typename ReduceTile<Fn>::S;
 
 template <class Fn, typename TS>
-__global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<Fn::NIN, Fn::NOUT> p) {
+__global__ void __launch_bounds__(kBlock, MinBlocks<Fn>::value) reduce2d_kernel(const Reduce2DParams<Fn::NIN, Fn::NOUT> p) {
   using T = typename Fn::T;
   using S = ReduceStage<Fn>;
+  constexpr int TR = ReduceTile<Fn>::TR;
   constexpr int NIN = Fn::NIN, NOUT = Fn::NOUT, R = Fn::R;
   constexpr int EPT = S::EPT, TILE = S::TILE;
   constexpr int RR = R > 1 ? R : 1;
   constexpr bool AUX = HasAux<Fn>::value;
   constexpr int N0 = HasAux<Fn>::N0, N1 = HasAux<Fn>::N1;
   extern __shared__ __align__(16) unsigned char s_dyn[];
-  __shared__ int s_cnt[RR], s_base[RR + 1];
+  __shared__ int s_cnt[RR], s_base[RR + 1], s_next;
   __shared__ double s_red[kBlock / 32][kTC];
-  __shared__ double s_aux0[AUX ? kTR * N0 : 1], s_aux1[AUX ? kTR * N1 : 1];
+  __shared__ double s_aux0[AUX ? TR * N0 : 1], s_aux1[AUX ? TR * N1 : 1];
+  __shared__ T s_val0[AUX ? TR : 1], s_val1[AUX ? TR : 1];
+  using RT = ReduceTile<Fn>;
   T* buf;
   uint16_t* list;
   uint8_t* regs;
@@ -412,17 +456,24 @@ __global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<F
 
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t rt = t / p.n_col_tiles, ct = t % p.n_col_tiles;
-    const int64_t r0 = rt * kTR, c0 = ct * kTC;
+    const int64_t r0 = rt * TR, c0 = ct * kTC;
     if constexpr (AUX) {
-      // Tables for this tile: warp 0 fills input AUX_IN0's, warp 1 AUX_IN1's.
-      const int which = warp, mode = which == 0 ? mode0 : mode1;
-      if (which < 2 && mode != 0) {
-        const int64_t r = mode == 1 ? r0 + lane : r0, c = mode == 1 ? c0 : c0 + lane;
+      // Tables for this tile: entries [0, TR) are input AUX_IN0's, [TR, 2TR)
+      // input AUX_IN1's; a row table has TR entries, a column table kTC.
+      for (int e = tid; e < 2 * TR; e += kBlock) {
+        const int which = e / TR, j = e % TR, mode = which == 0 ? mode0 : mode1;
+        if (mode == 0 || (mode == 2 && j >= kTC)) continue;
+        const int64_t r = mode == 1 ? r0 + j : r0, c = mode == 1 ? c0 : c0 + j;
         if (r < p.rows && c < p.cols) {
           const int q = which == 0 ? Fn::AUX_IN0 : Fn::AUX_IN1;
           const T v = load_as<TS, T>(p.in_ptr[q] + (r * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
-          if (which == 0) Fn::make_aux0(v, s_aux0 + lane * N0);
-          else Fn::make_aux1(v, s_aux1 + lane * N1);
+          if (which == 0) {
+            s_val0[j] = v;
+            Fn::make_aux0(v, s_aux0 + j * N0);
+          } else {
+            s_val1[j] = v;
+            Fn::make_aux1(v, s_aux1 + j * N1);
+          }
         }
       }
       __syncthreads();
@@ -442,15 +493,45 @@ __global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<F
         else if constexpr (R > 1) reg[k] = Fn::classify(v);
         else reg[k] = 0;
 #pragma unroll
-        for (int q = 0; q < NIN; ++q) buf[q * TILE + li] = v[q];
+        for (int q = 0; q < NIN; ++q)
+          if (RT::slot(q) >= 0) buf[RT::slot(q) * TILE + li] = v[q];
       }
     }
     if constexpr (AUX) {
-      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base);
-      cta_eval_sorted_aux<Fn, TILE>(count, buf, list, regs, p.out_mask, s_aux0, mode0, s_aux1, mode1);
+      // As cta_eval_groups, with the table inputs taken from their tables.
+      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base, &s_next);
+      const int ngroups = (count + 31) >> 5;
+      for (;;) {
+        int gidx = 0;
+        if (lane == 0) gidx = atomicAdd(&s_next, 1);
+        gidx = __shfl_sync(0xffffffffu, gidx, 0);
+        if (gidx >= ngroups) break;
+        const int j = (gidx << 5) + lane;
+        if (j < count) {
+          const int li = list[j];
+          const int lr = li / kTC, lc = li % kTC;
+          T v[NIN], o[NOUT];
+#pragma unroll
+          for (int q = 0; q < NIN; ++q)
+            if (RT::slot(q) >= 0) v[q] = buf[RT::slot(q) * TILE + li];
+#pragma unroll
+          for (int which = 0; which < 2; ++which) {
+            const int q = which == 0 ? Fn::AUX_IN0 : Fn::AUX_IN1, mode = which == 0 ? mode0 : mode1;
+            const T* tab = which == 0 ? s_val0 : s_val1;
+            v[q] = mode == 1 ? tab[lr]
+                 : mode == 2 ? tab[lc]
+                             : load_as<TS, T>(p.in_ptr[q] + ((r0 + lr) * p.in_s0[q] + (c0 + lc) * p.in_s1[q]) *
+                                                                (int64_t)sizeof(TS));
+          }
+          Fn::eval(regs[li], v, o, p.out_mask, aux_at<N0>(s_aux0, mode0, li), aux_at<N1>(s_aux1, mode1, li));
+#pragma unroll
+          for (int q = 0; q < NOUT; ++q) buf[q * TILE + li] = o[q];
+        }
+      }
+      __syncthreads();
     } else if constexpr (R > 1) {
-      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base);
-      cta_eval_sorted<Fn, TILE>(count, buf, list, regs, p.out_mask);
+      const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base, &s_next);
+      cta_eval_groups<Fn, TILE, false>(count, buf, list, regs, p.out_mask, &s_next, nullptr, 0, nullptr, 0);
     } else {
 #pragma unroll
       for (int k = 0; k < EPT; ++k) {
@@ -467,7 +548,7 @@ __global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<F
       __syncthreads();
     }
 
-    const int rows_here = (int)(p.rows - r0 < (int64_t)kTR ? p.rows - r0 : (int64_t)kTR);
+    const int rows_here = (int)(p.rows - r0 < (int64_t)TR ? p.rows - r0 : (int64_t)TR);
     const int cols_here = (int)(p.cols - c0 < (int64_t)kTC ? p.cols - c0 : (int64_t)kTC);
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
@@ -486,7 +567,7 @@ __global__ void __launch_bounds__(kBlock) reduce2d_kernel(const Reduce2DParams<F
         // Row sums: warp w takes rows w, w+8, ...; lane = column; fixed
         // shuffle tree.
         double tile_sum = 0.0;
-        for (int lr = warp; lr < kTR; lr += kBlock / 32) {
+        for (int lr = warp; lr < TR; lr += kBlock / 32) {
           double v = (lr < rows_here && lane < cols_here) ? (double)buf[o * TILE + lr * kTC + lane] : 0.0;
 #pragma unroll
           for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
