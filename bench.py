@@ -441,6 +441,140 @@ def reference_arm(args):
     )
 
 
+
+# ------------------------------------------------------- secondary workloads
+def _peak_hbm():
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _rate(fn, n, steps, warmup, flush):
+    """Gelem/s of fn over n elements (CUDA events per call, L2 flushed between calls)."""
+    return n * steps / timed_steps(fn, steps, warmup, flush) / 1e9
+
+
+def _max_rel(lo, hi, floor=1e-30):
+    lo, hi = lo.double(), hi.double()
+    m = torch.isfinite(lo) & torch.isfinite(hi) & (hi.abs() > floor) & (hi.abs() < 1e30)
+    return ((lo - hi).abs() / hi.abs())[m].max().item() if bool(m.any()) else 0.0
+
+
+def secondary_arm(args):
+    """The other benchmark configurations (parity-test cases of the path), timed
+    the same way; one JSON line with one entry per function."""
+    from torchscience_b200 import special_functions as sf
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    gen = torch.Generator(device=dev).manual_seed(0)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    S, W = args.steps, args.warmup
+    peak, peak_src = _peak_hbm()
+    res = {}
+
+    def U(n, lo, hi, dtype=torch.float64):
+        return (torch.rand(n, generator=gen, device=dev, dtype=torch.float64) * (hi - lo) + lo).to(dtype)
+
+    def LU(n, lo, hi, dtype=torch.float64):
+        return torch.exp(U(n, math.log(lo), math.log(hi))).to(dtype)
+
+    if args.workload == "c1":
+        desc = "log_gamma and bessel_j_0 FP64 forward, x ~ U(0.01, 50), contiguous"
+        for n in (1 << 20, 1 << 28):
+            x = U(n, 0.01, 50.0)
+            for name in ("log_gamma", "bessel_j_0"):
+                fn = getattr(sf, name)
+                r = _rate(lambda: fn(x), n, S, W, flush)
+                res[f"{name}_2^{int(math.log2(n))}"] = {
+                    "fwd_gelem_s": r, "hbm_gbs": 16 * r, "hbm_frac": 16 * r / peak}
+            del x
+    elif args.workload == "c3":
+        n = 1 << 26
+        desc = "bessel J/Y/I/K, nu ~ U(0, 20), x ~ LogU(1e-3, 1e3), 2^26 elements; fwd and fwd + d/dx"
+        nu64, x64 = U(n, 0.0, 20.0), LU(n, 1e-3, 1e3)
+        nu32, x32 = nu64.float(), x64.float()
+        g32 = torch.randn(n, generator=gen, device=dev, dtype=torch.float32)
+        for name in ("bessel_j", "bessel_y", "modified_bessel_i", "modified_bessel_k"):
+            fn = getattr(sf, name)
+            row = {}
+            for tag, nu, x, g in (("mixed", nu32, x32, g32), ("fp64", nu32.double(), x32.double(), g32.double())):
+                xr = x.clone().requires_grad_(True)
+
+                def fb():
+                    y = fn(nu, xr)
+                    torch.autograd.grad(y, xr, g)
+
+                with torch.no_grad():
+                    row[f"{tag}_fwd_gelem_s"] = _rate(lambda: fn(nu, x), n, S, W, flush)
+                row[f"{tag}_fwd_bwd_gelem_s"] = _rate(fb, n, S, W, flush)
+            with torch.no_grad():
+                row["mixed_max_rel_err_vs_fp64"] = _max_rel(fn(nu32, x32), fn(nu32.double(), x32.double()))
+            row["mixed_speedup_fwd_bwd"] = row["mixed_fwd_bwd_gelem_s"] / row["fp64_fwd_bwd_gelem_s"]
+            res[name] = row
+    elif args.workload == "c4":
+        n = 1 << 24
+        desc = ("hypergeometric_2_f_1, a, b ~ U(-10, 10), c ~ U(-10, 10) (|c - round c| >= 1e-3 for c <= 0), "
+                "z ~ U(-5, 0.9) w.p. 0.9 else U(0.9, 0.999), 2^24 elements; fwd and fwd + all four grads")
+        a, b, c = U(n, -10, 10), U(n, -10, 10), U(n, -10, 10)
+        bad = (c <= 0) & ((c - c.round()).abs() < 1e-3)
+        c = torch.where(bad, c + 0.5, c)
+        z = torch.where(torch.rand(n, generator=gen, device=dev) < 0.9, U(n, -5.0, 0.9), U(n, 0.9, 0.999))
+        g = torch.randn(n, generator=gen, device=dev, dtype=torch.float64)
+        for tag, dt in (("fp64", torch.float64), ("mixed", torch.float32)):
+            ins = [t.to(dt) for t in (a, b, c, z)]
+            req = [t.clone().requires_grad_(True) for t in ins]
+
+            def fb():
+                y = sf.hypergeometric_2_f_1(*req)
+                torch.autograd.grad(y, req, g.to(dt))
+
+            with torch.no_grad():
+                res[f"{tag}_fwd_gelem_s"] = _rate(lambda: sf.hypergeometric_2_f_1(*ins), n, S, W, flush)
+            res[f"{tag}_fwd_bwd_gelem_s"] = _rate(fb, n, S, W, flush)
+    elif args.workload == "c5":
+        desc = ("Gamma log-likelihood sum over 2^28 elements, k ~ LogU(0.1, 100), theta ~ LogU(0.1, 10), "
+                "x ~ Gamma(k, theta); fwd + grads (autograd) + HVP in k (double backward); "
+                "K(m), E(m), m ~ U(0, 1 - 1e-9), 2^26 elements, fwd + d/dm")
+        n = 1 << 28
+        k, th = LU(n, 0.1, 100.0, torch.float32), LU(n, 0.1, 10.0, torch.float32)
+        torch.manual_seed(0)
+        x = torch.distributions.Gamma(k, 1.0 / th).sample().clamp_min(1e-30)
+        v = torch.randn(n, generator=gen, device=dev, dtype=torch.float32)
+        for tag, dt in (("mixed", torch.float32), ("fp64", torch.float64)):
+            kk, tt, xx, vv = (t.to(dt) for t in (k, th, x, v))
+            kr, tr = kk.clone().requires_grad_(True), tt.clone().requires_grad_(True)
+
+            def step():
+                L = ((kr - 1) * torch.log(xx) - xx / tr - sf.log_gamma(kr) - kr * torch.log(tr)).sum()
+                gk, gt = torch.autograd.grad(L, (kr, tr), create_graph=True)
+                torch.autograd.grad(gk, kr, vv)
+
+            res[f"likelihood_{tag}_fwd_bwd_hvp_gelem_s"] = _rate(step, n, S, W, flush)
+            del kk, tt, xx, vv, kr, tr
+            torch.cuda.empty_cache()
+        del k, th, x, v
+        m = U(1 << 26, 0.0, 1.0 - 1e-9, torch.float32)
+        for name in ("complete_legendre_elliptic_integral_k", "complete_legendre_elliptic_integral_e"):
+            fn = getattr(sf, name)
+            for tag, mm in (("mixed", m), ("fp64", m.double())):
+                mr = mm.clone().requires_grad_(True)
+
+                def fb():
+                    y = fn(mr)
+                    torch.autograd.grad(y, mr, torch.ones_like(mr))
+
+                with torch.no_grad():
+                    res[f"{name}_{tag}_fwd_gelem_s"] = _rate(lambda: fn(mm), mm.numel(), S, W, flush)
+                res[f"{name}_{tag}_fwd_bwd_gelem_s"] = _rate(fb, mm.numel(), S, W, flush)
+    print(json.dumps({
+        "metric": METRIC, "workload": args.workload, "unit": "Gelem/s", "steps": S, "warmup": W,
+        "data": "synthetic, seeded on the device", "config": {"workload": desc, "l2": "flushed between steps"},
+        "peak_hbm_gbs": peak, "peak_source": peak_src, "results": res}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -448,11 +582,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument(
+        "--workload", choices=["p_grid", "c1", "c3", "c4", "c5"], default="p_grid",
+        help="p_grid (default): the headline P(a, x) workload; c1/c3/c4/c5: the other configurations, one GPU")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload != "p_grid":
+        secondary_arm(args)
     else:
         our_arm(args)
 
