@@ -150,6 +150,15 @@ def timed_steps(fn, steps, warmup, flush):
     return total
 
 
+def max_over_ranks(values, dist, device):
+    """Each timing as the maximum over ranks (the job ends with its slowest
+    shard); `dist` is torch.distributed, or None for a single process."""
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def count_launches(fn) -> int:
     """Kernels this library launches in one call of fn, read from the
     library's own launch counter (tsb_launch_count)."""
@@ -295,10 +304,7 @@ def our_arm(args):
     launches_per_step = count_launches(step64)
     k_sec, k_bytes = kernel_roofline([t.detach() for t in d64], max(args.steps, 5), flush)
 
-    times = torch.tensor([t_fb, t_f, t_fb32, t_f32, t_e2e], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    t_fb, t_f, t_fb32, t_f32, t_e2e = times.tolist()
+    t_fb, t_f, t_fb32, t_f32, t_e2e = max_over_ranks([t_fb, t_f, t_fb32, t_f32, t_e2e], dist, dev)
     n = world
     total = ELEMS * args.steps * n
     result = {
