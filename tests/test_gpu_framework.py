@@ -104,3 +104,36 @@ def test_c_abi_reports_launch_errors_as_status_not_crash():
     dout[0].sizes[0], dout[0].strides[0] = 16, 1
     st = lib().tsb_log_gamma(din, 1, dout, 1, 0, None, ctypes.c_int64(0), None)
     assert st == -1 and b"misaligned" in lib().tsb_last_error()
+
+
+@pytest.mark.parametrize("op", ["bessel_j", "modified_bessel_k", "regularized_gamma_p"])
+def test_gradient_of_one_input_only(op):
+    """Only the second input requires grad (the common case for Bessel
+    functions of a fixed order): the first input's gradient is neither
+    computed nor returned, and the second matches the full backward."""
+    import numpy as np
+
+    from torchscience_b200 import special_functions as sf
+
+    fn = getattr(sf, op)
+    first = torch.tensor([0.5, 1.5, 2.25, 3.0], dtype=torch.float64, device="cuda")
+    second = torch.tensor([0.3, 1.7, 4.2, 9.0], dtype=torch.float64, device="cuda", requires_grad=True)
+    y = fn(first, second)
+    (g,) = torch.autograd.grad(y.sum(), second)
+    full = getattr(torch.ops.torchscience, op + "_backward")(torch.ones_like(y), first, second.detach())
+    np.testing.assert_array_equal(g.cpu().numpy(), full[1].cpu().numpy())
+    first_rg = first.clone().requires_grad_(True)
+    y2 = fn(first_rg, second.detach())
+    (g2,) = torch.autograd.grad(y2.sum(), first_rg)
+    assert torch.isfinite(g2).all()
+
+
+def test_hyp2f1_gradient_of_z_only():
+    from torchscience_b200 import special_functions as sf
+
+    a = torch.tensor([0.7, 1.3], dtype=torch.float64, device="cuda")
+    z = torch.tensor([0.2, -1.5], dtype=torch.float64, device="cuda", requires_grad=True)
+    y = sf.hypergeometric_2_f_1(a, a + 0.5, a + 2.0, z)
+    (gz,) = torch.autograd.grad(y.sum(), z, create_graph=True)
+    (gzz,) = torch.autograd.grad(gz.sum(), z)
+    assert torch.isfinite(gz).all() and torch.isfinite(gzz).all()

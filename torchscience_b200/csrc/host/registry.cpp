@@ -30,6 +30,15 @@ inline bool any_cuda(std::initializer_list<at::Tensor> ts) {
   return false;
 }
 
+// An autograd Function cannot return undefined tensors: gradients that were
+// not requested (and so not computed) come back as a zero expanded to the
+// input's shape, which allocates one element.
+inline torch::autograd::variable_list defined_or_zero(std::vector<at::Tensor> r, at::TensorList like) {
+  for (size_t i = 0; i < r.size(); ++i)
+    if (!r[i].defined()) r[i] = at::zeros({}, like[i].options()).expand(like[i].sizes());
+  return r;
+}
+
 }  // namespace tsbh
 
 // ---------------------------------------------------------------- unary ops
@@ -178,7 +187,7 @@ inline bool any_cuda(std::initializer_list<at::Tensor> ts) {
       at::AutoDispatchBelowAutograd guard;                                                             \
       if (any_cuda({g, a, b})) {                                                                       \
         /* Gradients come back already reduced to a's and b's shapes. */                               \
-        return run_reduced_backward(BWD, #name "_backward", g, {a, b}, {ra, rb});                      \
+        return defined_or_zero(run_reduced_backward(BWD, #name "_backward", g, {a, b}, {ra, rb}), {a, b}); \
       }                                                                                                 \
       static auto op = c10::Dispatcher::singleton()                                                    \
                            .findSchemaOrThrow("torchscience::" #name "_backward", "")                  \
@@ -335,8 +344,9 @@ class Hypergeometric2F1Backward : public torch::autograd::Function<Hypergeometri
     at::AutoDispatchBelowAutograd guard;
     if (any_cuda({g, a, b, c, z})) {
       /* Gradients come back already reduced to the inputs' shapes. */
-      return run_reduced_backward(tsb_hypergeometric_2_f_1_backward, "hypergeometric_2_f_1_backward", g,
-                                  {a, b, c, z}, want);
+      return defined_or_zero(run_reduced_backward(tsb_hypergeometric_2_f_1_backward, "hypergeometric_2_f_1_backward",
+                                                  g, {a, b, c, z}, want),
+                             {a, b, c, z});
     }
     static auto op = c10::Dispatcher::singleton()
                          .findSchemaOrThrow("torchscience::hypergeometric_2_f_1_backward", "")

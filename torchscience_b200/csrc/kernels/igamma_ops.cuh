@@ -19,7 +19,11 @@ namespace tsb {
 __device__ __forceinline__ double igamma_px_only(double a, double x, const IgPre& P) {
   if (isnan(a) || isnan(x) || x < 0.0 || a <= 0.0) return CUDART_NAN;
   if (x == 0.0 || isinf(x) || isinf(a)) return 0.0;
-  return exp(igamma_log_prefix_d(a, x, P) + (P.la() - P.lx()));
+  // the same expressions as the full backward (igamma_eval_d), branch by branch
+  const double lnD = igamma_log_prefix_d(a, x, P);
+  if (x < a + 1.0) return igamma_px_from(exp(lnD), lnD, a, P);
+  const double lnE = lnD + P.la();
+  return lnE > -700.0 ? exp(lnE) * P.rx() : exp(lnE - P.lx());
 }
 
 // Every functor here keeps per-row / per-column tables of its a and x inputs
