@@ -175,9 +175,12 @@ def test_gradcheck_and_gradgradcheck():
 
 
 def test_grad_z_alone_matches_full_backward():
+    """grad_z alone is (ab/c) 2F1(a+1, b+1; c+1; z) (one value evaluation);
+    with the other grads it comes from the same pass as they do.  Both agree
+    to the gradient bound."""
     t = [cuda(v[:500]) for v in (A, B, C, Z)]
     g = cuda(np.ones(500))
     gz = torch.empty_like(g)
     assert call("hypergeometric_2_f_1_backward", [g, *t], [None, None, None, gz]) == 0
     full = run("hypergeometric_2_f_1_backward", g, *t, n_out=4)[3]
-    torch.testing.assert_close(gz, full, rtol=0, atol=0)
+    torch.testing.assert_close(gz, full, rtol=2e-9, atol=0)

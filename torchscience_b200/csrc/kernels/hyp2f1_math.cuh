@@ -23,7 +23,9 @@
 // evaluated at shifted c and extrapolated back.
 // Derivatives in a, b, c are analytic in all cases: term-wise series
 // derivatives (harmonic sums Σ 1/(p + k)) and, in the connection formula,
-// derivatives of its Γ-ratios through ψ.  ∂/∂z = (ab/c) 2F1(a+1, b+1; c+1; z).
+// derivatives of its Γ-ratios through ψ.  ∂/∂z comes from the same pass
+// (d t_k/dx = k t_k/x, and the chain rule through the transformations); at
+// the special points and for grad_z alone it is (ab/c) 2F1(a+1, b+1; c+1; z).
 // Second derivatives in a, b, c are Richardson-extrapolated central
 // differences of the analytic gradient (evaluator held fixed); those in z come
 // from the gradient of 2F1(a+1, b+1; c+1; z).  At the special points the
@@ -69,29 +71,36 @@ __device__ inline void rgamma_dd(double x, double& r, double& dr) {
 }
 
 // Σ_k (p)_k (q)_k / ((c)_k k!) x^k with Σ|terms| and, if DERIVS, the
-// derivatives in p, q, c.  Convergence is tested only once k is past
-// max(|p|, |q|), against the absolute sums (the attainable accuracy).
+// derivatives in p, q, c and x (d t_k / dx = k t_k / x).  Convergence is
+// tested only once k is past max(|p|, |q|), against the absolute sums (the
+// attainable accuracy).
 struct H2Sum {
   double s, abs, last;
-  double dp, dq, dc;
+  double dp, dq, dc, dx;
   bool conv;
 };
 template <bool DERIVS>
 __device__ __noinline__ H2Sum h2f1_sum(double p, double q, double c, double x, int max_terms) {
   H2Sum r;
   double t = 1.0, s = 1.0, A = 1.0, hp = 0.0, hq = 0.0, hc = 0.0;
-  double dp = 0.0, dq = 0.0, dc = 0.0, Ap = 0.0, Aq = 0.0, Ac = 0.0;
+  double dp = 0.0, dq = 0.0, dc = 0.0, Ap = 0.0, Aq = 0.0, Ac = 0.0, kt = 0.0;
   const double kmin = fmax(fabs(p), fabs(q)) + 2.0;
   r.conv = false;
   for (int k = 0; k < max_terms; ++k) {
     const double fk = (double)k;
     const double pk = p + fk, qk = q + fk, ck = c + fk;
     if (DERIVS) {
-      hp += 1.0 / pk;
-      hq += 1.0 / qk;
-      hc += 1.0 / ck;
+      // one reciprocal per term: r = 1/(pk qk ck (k+1)) gives 1/pk, 1/qk, 1/ck
+      // and the term ratio pk qk/(ck (k+1)) = (pk qk)^2 r
+      const double pq = pk * qk, ck1 = ck * (fk + 1.0);
+      const double r = 1.0 / (pq * ck1);
+      hp = fma(qk * ck1, r, hp);
+      hq = fma(pk * ck1, r, hq);
+      hc = fma(pq * (fk + 1.0), r, hc);
+      t *= pq * pq * r * x;
+    } else {
+      t *= pk * qk / (ck * (fk + 1.0)) * x;
     }
-    t *= pk * qk / (ck * (fk + 1.0)) * x;
     s += t;
     A += fabs(t);
     if (DERIVS) {
@@ -99,6 +108,7 @@ __device__ __noinline__ H2Sum h2f1_sum(double p, double q, double c, double x, i
       dp += tp;
       dq += tq;
       dc -= tc;
+      kt = fma(fk + 1.0, t, kt);
       Ap += fabs(tp);
       Aq += fabs(tq);
       Ac += fabs(tc);
@@ -118,12 +128,14 @@ __device__ __noinline__ H2Sum h2f1_sum(double p, double q, double c, double x, i
   r.dp = dp;
   r.dq = dq;
   r.dc = dc;
+  r.dx = DERIVS ? (x != 0.0 ? kt / x : p * q / c) : 0.0;
   return r;
 }
 
-// G(p, q; c; x) with an error estimate and, if DERIVS, its p-, q-, c-derivatives.
+// G(p, q; c; x) with an error estimate and, if DERIVS, its p-, q-, c- and
+// x-derivatives.
 struct H2Val {
-  double v, err, dp, dq, dc;
+  double v, err, dp, dq, dc, dx;
 };
 
 // Direct series; the estimate adds the truncated tail when not converged.
@@ -136,6 +148,7 @@ __device__ inline H2Val h2f1_direct(double p, double q, double c, double x, int 
   r.dp = S.dp;
   r.dq = S.dq;
   r.dc = S.dc;
+  r.dx = S.dx;
   return r;
 }
 
@@ -164,7 +177,7 @@ __device__ __noinline__ H2Val h2f1_connect(double p, double q, double c, double 
   H2Sum S1, S2;
   S1.s = S2.s = 1.0;
   S1.abs = S2.abs = 1.0;
-  S1.dp = S1.dq = S1.dc = S2.dp = S2.dq = S2.dc = 0.0;
+  S1.dp = S1.dq = S1.dc = S1.dx = S2.dp = S2.dq = S2.dc = S2.dx = 0.0;
   S1.conv = S2.conv = true;
   if (G1 != 0.0 || DERIVS) S1 = h2f1_sum<DERIVS>(p, q, 1.0 - s, y, kH2ConnTerms);
   if (G2 != 0.0 || DERIVS) S2 = h2f1_sum<DERIVS>(u, v, 1.0 + s, y, kH2ConnTerms);
@@ -174,8 +187,10 @@ __device__ __noinline__ H2Val h2f1_connect(double p, double q, double c, double 
   // tgamma and the prefactor products add a few ulp to each term
   r.err = 8.0 * kH2Ulp * (fabs(G1) * S1.abs + fabs(G2 * Y) * S2.abs);
   if (!isfinite(r.v) || !(S1.conv || G1 == 0.0) || !(S2.conv || G2 == 0.0)) r.err = CUDART_INF;
-  r.dp = r.dq = r.dc = 0.0;
+  r.dp = r.dq = r.dc = r.dx = 0.0;
   if (DERIVS) {
+    // d/dx = -d/dy: G1 S1'(y) + G2 y^s (s/y S2 + S2'(y))
+    r.dx = -(G1 * S1.dx + G2 * Y * (s / y * S2.s + S2.dx));
     // s_p = s_q = -1, s_c = 1; u_p = -1, u_c = 1; v_q = -1, v_c = 1.
     const double psc = digamma_d(c), pss = digamma_d(s), psms = digamma_d(-s);
     const double gg1 = gc * gs, gg2 = gc * gms;
@@ -213,6 +228,7 @@ __device__ inline H2Val h2f1_connect_shifted(double p, double q, double c, doubl
   r.dp = (2.0 * (r1.dp + r2.dp) - 0.5 * (r3.dp + r4.dp)) / 3.0;
   r.dq = (2.0 * (r1.dq + r2.dq) - 0.5 * (r3.dq + r4.dq)) / 3.0;
   r.dc = (2.0 * (r1.dc + r2.dc) - 0.5 * (r3.dc + r4.dc)) / 3.0;
+  r.dx = (2.0 * (r1.dx + r2.dx) - 0.5 * (r3.dx + r4.dx)) / 3.0;
   r.err = 2.0 * (r1.err + r2.err + r3.err + r4.err);
   return r;
 }
@@ -414,28 +430,20 @@ struct H2f1Grad {
   double v, da, db, dc, dz;
 };
 
-// Value and (a, b, c) derivatives by the evaluator and Pfaff variant of a plan
-// (the plan's p, q are recomputed from a, b, c; x and lz depend on z only).
-static __device__ __noinline__ H2f1Grad h2f1_param_grad(const H2Plan& plan, double a, double b, double c, double z) {
-  H2Plan P = plan;
-  if (P.pfaff) {
-    h2f1_set_swap(P, a, b, c, plan.swap);
-  } else {
-    P.p = a;
-    P.q = b;
-  }
-  const H2Val G = h2f1_core<true>(P.method, P.p, P.q, c, P.x);
+// F and its gradient from G(p, q; c; x) and G's derivatives, for a plan.
+// Pfaff: F = (1-z)^-p G, x = z/(z-1), p = a, q = c - b (or p = b, q = c - a);
+// dF/dz = p F/(1-z) - (1-z)^-p G'(x)/(1-z)^2.
+__device__ inline H2f1Grad h2f1_assemble(const H2Plan& P, const H2Val& G, double z) {
   H2f1Grad g;
-  g.dz = 0.0;
   if (!P.pfaff) {
     g.v = G.v;
     g.da = G.dp;
     g.db = G.dq;
     g.dc = G.dc;
+    g.dz = G.dx;
     return g;
   }
-  // F = (1-z)^-p G(p, q; c; x): p = a, q = c - b (or p = b, q = c - a).
-  const double pre = exp(-P.p * P.lz);
+  const double pre = exp(-P.p * P.lz), omz = 1.0 - z;
   g.v = pre * G.v;
   const double Fp = pre * (G.dp - P.lz * G.v), Fq = pre * G.dq;
   g.dc = pre * (G.dq + G.dc);
@@ -446,7 +454,21 @@ static __device__ __noinline__ H2f1Grad h2f1_param_grad(const H2Plan& plan, doub
     g.db = Fp;
     g.da = -Fq;
   }
+  g.dz = P.p / omz * g.v - pre * G.dx / (omz * omz);
   return g;
+}
+
+// Value and derivatives by the evaluator and Pfaff variant of a plan (the
+// plan's p, q are recomputed from a, b, c; x and lz depend on z only).
+static __device__ __noinline__ H2f1Grad h2f1_param_grad(const H2Plan& plan, double a, double b, double c, double z) {
+  H2Plan P = plan;
+  if (P.pfaff) {
+    h2f1_set_swap(P, a, b, c, plan.swap);
+  } else {
+    P.p = a;
+    P.q = b;
+  }
+  return h2f1_assemble(P, h2f1_core<true>(P.method, P.p, P.q, c, P.x), z);
 }
 
 __device__ inline double h2f1_dz(double a, double b, double c, double z, double eps = kH2f1Eps) {
@@ -472,25 +494,47 @@ __device__ inline void h2f1_fd_grad(double a, double b, double c, double z, H2f1
 }
 
 // Full gradient (∂/∂a, ∂/∂b, ∂/∂c, ∂/∂z), with the region and plan used.
+// Away from the special points it takes one evaluation with derivatives
+// whenever the first evaluator is accurate (the common case); otherwise the
+// evaluator is chosen as for the value (h2f1_eval) and evaluated again.
 static __device__ __noinline__ H2f1Grad h2f1_grad(double a, double b, double c, double z, double eps = kH2f1Eps,
                                                   int* region_out = nullptr, H2Plan* plan_out = nullptr) {
   H2f1Grad g;
   double sv;
-  g.dz = h2f1_dz(a, b, c, z, eps);
   if (h2f1_special(a, b, c, z, sv, eps)) {
     g.v = sv;
+    g.dz = h2f1_dz(a, b, c, z, eps);
     h2f1_fd_grad(a, b, c, z, g, eps);
     if (region_out) *region_out = kH2Special;
     return g;
   }
   const int region = h2f1_region_of(z);
-  H2Plan plan;
-  h2f1_eval(region, a, b, c, z, &plan);
-  const double dz = g.dz;
-  g = h2f1_param_grad(plan, a, b, c, z);
-  g.dz = dz;
+  H2Plan P = h2f1_plan(region, a, b, c, z);
+  H2Val G;
+  bool ok;
+  if (P.method == kH2mSeries) {
+    G = h2f1_direct<true>(P.p, P.q, c, P.x, kH2ConnTerms);
+    if (P.pfaff && !(G.err <= 64.0 * kH2Ulp * fabs(G.v))) {
+      H2Plan Q = P;
+      h2f1_set_swap(Q, a, b, c, !P.swap);
+      const H2Val GQ = h2f1_direct<true>(Q.p, Q.q, c, Q.x, kH2ConnTerms);
+      if (GQ.err / fabs(GQ.v) < G.err / fabs(G.v)) {
+        G = GQ;
+        P = Q;
+      }
+    }
+    ok = true;
+  } else {
+    G = h2f1_connect<true>(P.p, P.q, c, 1.0 - P.x);
+    ok = G.err <= 64.0 * kH2Ulp * fabs(G.v);
+  }
+  if (!ok) {
+    h2f1_eval(region, a, b, c, z, &P);
+    G = h2f1_core<true>(P.method, P.p, P.q, c, P.x);
+  }
+  g = h2f1_assemble(P, G, z);
   if (region_out) *region_out = region;
-  if (plan_out) *plan_out = plan;
+  if (plan_out) *plan_out = P;
   return g;
 }
 

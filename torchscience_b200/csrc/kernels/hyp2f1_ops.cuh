@@ -10,6 +10,13 @@
 #include "dispatch.cuh"
 #include "hyp2f1_math.cuh"
 
+// Resident CTAs the forward and backward register allocation must allow: 4
+// (64 registers, with spills) measured 25% faster forward and 15% faster
+// backward than the unconstrained allocation (122 / 200 registers).
+#ifndef TSB_H2_MINB
+#define TSB_H2_MINB 4
+#endif
+
 namespace tsb {
 
 // The reference's special-case tolerance for the data type (hyp2f1_epsilon).
@@ -21,6 +28,7 @@ __device__ constexpr double h2f1_eps_for() {
 template <typename T_>
 struct Hyp2f1Fwd {
   using T = T_;
+  static constexpr int MIN_BLOCKS = TSB_H2_MINB;
   static constexpr int NIN = 4, NOUT = 1, R = kH2Regions;
   static constexpr bool REDUCE = false;
   __device__ static int classify(const T* in) {
@@ -41,6 +49,7 @@ struct Hyp2f1Fwd {
 template <typename T_>
 struct Hyp2f1Bwd {
   using T = T_;
+  static constexpr int MIN_BLOCKS = TSB_H2_MINB;
   static constexpr int NIN = 5, NOUT = 4, R = kH2Regions;
   static constexpr bool REDUCE = true;
   __device__ static int classify(const T* in) {

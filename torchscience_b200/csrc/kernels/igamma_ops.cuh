@@ -8,6 +8,7 @@
 #include "dispatch.cuh"
 #include "igamma_math.cuh"
 
+// Resident CTAs the forward's register allocation must allow (64 registers).
 #ifndef TSB_IGF_MINB
 #define TSB_IGF_MINB 4
 #endif
