@@ -93,6 +93,30 @@ def test_mixed_within_1e6_of_fp64():
         assert e.max() <= 1e-6, f"mixed grad {k}: {e.max():.3e}"
 
 
+@pytest.mark.parametrize("upper", [False, True])
+def test_mixed_within_1e6_of_fp64_on_the_broadcast_grid(upper):
+    """Every element of a 1024 x 1024 grid of the benchmark distribution, as a
+    broadcast (the per-row/column-table path) and element by element:
+    P or Q and both derivatives, mixed against FP64 at the same float values."""
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    lu = lambda shape, lo, hi: torch.exp(  # noqa: E731
+        torch.rand(shape, generator=gen, device="cuda", dtype=torch.float64) * (np.log(hi) - np.log(lo)) + np.log(lo))
+    a32, x32 = lu((1024, 1), 1e-2, 1e3).float(), lu((1, 1024), 1e-3, 2e3).float()
+    name = "regularized_gamma_q" if upper else "regularized_gamma_p"
+    g = torch.ones(1024, 1024, device="cuda")
+    A32, X32 = a32.expand(1024, 1024).contiguous(), x32.expand(1024, 1024).contiguous()
+    for aa, xx in ((a32, x32), (A32, X32)):
+        (vm,) = run(name, aa, xx)
+        (vd,) = run(name, aa.double(), xx.double())
+        gm = run(name + "_backward", g, aa, xx, n_out=2)
+        gd = run(name + "_backward", g.double(), aa.double(), xx.double(), n_out=2)
+        for got, want in ((vm, vd), (gm[0], gd[0]), (gm[1], gd[1])):
+            u, v = got.double().cpu().numpy(), want.cpu().numpy()
+            m = (np.abs(v) > 1e-30) & (np.abs(v) < 3e38)
+            e = rel_err(u, v)[m]
+            assert e.max() <= 1e-6, f"{name}: {e.max():.3e}"
+
+
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 def test_fused_reduced_gradients_match_full_gradients(dtype):
     """Config-2 broadcast layout (R,1) x (1,C): gradients reduced in-kernel

@@ -157,7 +157,9 @@ inline int occupancy_for(K kernel, int block, size_t smem, int dev) {
   static int cache[64];
   int* slot = dev >= 0 && dev < 64 ? &cache[dev] : nullptr;
   if (slot && *slot > 0) return *slot;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // Opt in whenever dynamic shared memory is used: the default limit is
+  // 48 KB minus the kernel's static shared memory.
+  if (smem > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int blocks = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, block, smem) != cudaSuccess || blocks < 1) {
     cudaGetLastError();

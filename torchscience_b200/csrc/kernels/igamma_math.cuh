@@ -74,14 +74,55 @@ enum IgammaAuxA : int {
   kIgA_LGF,     // lgammaf(a+1) in float (classification)
   kIgA_LAF,     // __logf(a)
   kIgA_LA1F,    // __logf(a+1)
+  kIgA_LGFF,    // float-float pairs (packed hi, lo) for the mixed kernels: kIgA_LG,
+  kIgA_LAFF,    //   ln a,
+  kIgA_PRFF,    //   ψ(a) + 1/a,
+  kIgA_PSFF,    //   ψ(a)
   kIgAuxA
 };
 enum IgammaAuxX : int {
   kIgX_LX = 0,  // ln x
   kIgX_RX,      // 1/x
   kIgX_LXF,     // __logf(x)
+  kIgX_LXFF,    // ln x as a packed float-float pair
   kIgAuxX
 };
+
+// Float-float numbers (hi + lo, |lo| <= ulp(hi)/2) for the mixed kernels'
+// prefactor: ln D = a ln x - x - lnΓ(a+1) cancels by up to ~1e4 in the
+// benchmark domain, which plain float cannot carry to 1e-6.  Error-free
+// transformations: TwoSum (Knuth) and the FMA product error.
+struct IgFF {
+  float hi, lo;
+};
+__device__ __forceinline__ IgFF ff_split(double v) {
+  const float hi = (float)v;
+  return IgFF{hi, (float)(v - (double)hi)};
+}
+__device__ __forceinline__ double ff_pack(double v) {
+  const IgFF f = ff_split(v);
+  return __longlong_as_double(((long long)__float_as_int(f.hi) << 32) | (unsigned int)__float_as_int(f.lo));
+}
+__device__ __forceinline__ IgFF ff_unpack(double d) {
+  const long long b = __double_as_longlong(d);
+  return IgFF{__int_as_float((int)(b >> 32)), __int_as_float((int)(b & 0xffffffffll))};
+}
+__device__ __forceinline__ IgFF ff_two_sum(float a, float b) {
+  const float s = a + b, bb = s - a;
+  return IgFF{s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ IgFF ff_add(IgFF x, IgFF y) {
+  const IgFF s = ff_two_sum(x.hi, y.hi);
+  return ff_two_sum(s.hi, s.lo + (x.lo + y.lo));
+}
+__device__ __forceinline__ IgFF ff_neg(IgFF x) { return IgFF{-x.hi, -x.lo}; }
+__device__ __forceinline__ IgFF ff_mul_f(IgFF x, float a) {
+  const float p = x.hi * a;
+  const float e = fmaf(x.lo, a, fmaf(x.hi, a, -p));
+  return ff_two_sum(p, e);
+}
+// exp(hi + lo) = exp(hi) (1 + lo) for |lo| << 1.
+__device__ __forceinline__ float ff_exp(IgFF x) { return expf(x.hi) * (1.0f + x.lo); }
 
 __device__ inline double igamma_lg(double a) {
   return a < 10.0 ? lgamma(a + 1.0) : 0.5 * log(2.0 * CUDART_PI * a) + stirling_mu_d(a);
@@ -98,11 +139,16 @@ __device__ inline void igamma_aux_a(double a, double* o) {
   o[kIgA_LGF] = lgammaf(af + 1.0f);
   o[kIgA_LAF] = __logf(af);
   o[kIgA_LA1F] = __logf(af + 1.0f);
+  o[kIgA_LGFF] = ff_pack(o[kIgA_LG]);
+  o[kIgA_LAFF] = ff_pack(o[kIgA_LA]);
+  o[kIgA_PRFF] = ff_pack(o[kIgA_PSI] + o[kIgA_RA]);
+  o[kIgA_PSFF] = ff_pack(o[kIgA_PSI]);
 }
 __device__ inline void igamma_aux_x(double x, double* o) {
   o[kIgX_LX] = log(x);
   o[kIgX_RX] = 1.0 / x;
   o[kIgX_LXF] = __logf((float)x);
+  o[kIgX_LXFF] = ff_pack(o[kIgX_LX]);
 }
 
 struct IgPre {
@@ -118,6 +164,11 @@ struct IgPre {
   __device__ float laf() const { return A ? (float)A[kIgA_LAF] : __logf((float)a); }
   __device__ float la1f() const { return A ? (float)A[kIgA_LA1F] : __logf((float)a + 1.0f); }
   __device__ double lx() const { return X ? X[kIgX_LX] : log(x); }
+  __device__ IgFF lgff() const { return A ? ff_unpack(A[kIgA_LGFF]) : ff_split(igamma_lg(a)); }
+  __device__ IgFF laff() const { return A ? ff_unpack(A[kIgA_LAFF]) : ff_split(log(a)); }
+  __device__ IgFF prff() const { return A ? ff_unpack(A[kIgA_PRFF]) : ff_split(digamma_d(a) + 1.0 / a); }
+  __device__ IgFF psff() const { return A ? ff_unpack(A[kIgA_PSFF]) : ff_split(digamma_d(a)); }
+  __device__ IgFF lxff() const { return X ? ff_unpack(X[kIgX_LXFF]) : ff_split(log(x)); }
   __device__ double rx() const { return X ? X[kIgX_RX] : 1.0 / x; }
   __device__ float lxf() const { return X ? (float)X[kIgX_LXF] : __logf((float)x); }
 };
@@ -283,28 +334,38 @@ struct IgammaOut {
 // iteration count, so the lanes of a warp run loops of similar length.
 enum IgammaRegion : int {
   // Numbered by decreasing cost (measured per element on B200), so that a
-  // tile's sorted list starts with its most expensive groups.
-  kIgS3 = 0,      // series, x/(a+1) < 1
-  kIgC2 = 1,      // continued fraction, x/(a+1) <= 1.5
-  kIgC1 = 2,      // continued fraction, x/(a+1) > 1.5
-  kIgS2 = 3,      // series, x/(a+1) < 0.7
-  kIgC0 = 4,      // continued fraction, x/(a+1) > 3
-  kIgS1 = 5,      // series, x/(a+1) < 0.35
-  kIgS0 = 6,      // series, x/(a+1) < 0.1
-  kIgSmallA = 7,  // a < 1, x < a + 1: series for P, dedicated formula for Q
-  kIgSat1 = 8,    // Q and every derivative underflow to 0 (P = 1)
-  kIgSat0 = 9,    // P and every derivative underflow to 0 (Q = 1)
-  kIgSpecial = 10,  // NaN / domain / x == 0 / x == inf
-  kIgRegions = 11
+  // tile's sorted list starts with its most expensive groups.  The cheap
+  // regions are split by the ratio that sets their iteration count, so that
+  // the lanes of a warp run loops of similar length.  The mixed forward also
+  // buckets the a < 1 continued fractions, which it runs in FP32 (kIgCa).
+  kIgS3 = 0,         // series, x/(a+1) < 1
+  kIgC2 = 1,         // continued fraction, x/(a+1) <= 1.5
+  kIgC1 = 2,         // continued fraction, x/(a+1) > 1.5
+  kIgS2 = 3,         // series, x/(a+1) < 0.7
+  kIgC0 = 4,         // continued fraction, 3 < x/(a+1) <= 10
+  kIgCa = 5,         // mixed forward only: continued fraction, a < 1 (FP32 there)
+  kIgS1 = 6,         // series, x/(a+1) < 0.35
+  kIgS0 = 7,         // series, 0.01 <= x/(a+1) < 0.1
+  kIgSmallA = 8,     // a < 1, 0.1 (a+1) <= x < a + 1: series for P, dedicated formula for Q
+  kIgC00 = 9,        // continued fraction, x/(a+1) > 10
+  kIgS00 = 10,       // series, x/(a+1) < 0.01
+  kIgSmallA0 = 11,   // a < 1, x < 0.1 (a+1)
+  kIgSat1 = 12,      // Q and every derivative underflow to 0 (P = 1)
+  kIgSat0 = 13,      // P and every derivative underflow to 0 (Q = 1)
+  kIgSpecial = 14,   // NaN / domain / x == 0 / x == inf
+  kIgRegions = 15
 };
 
 // Regions whose loops are short enough for FP32 accumulation (mixed kernels).
 __device__ __forceinline__ bool igamma_fp32_ok(int region) {
-  return region == kIgS0 || region == kIgS1 || region == kIgC0;
+  return region == kIgS00 || region == kIgS0 || region == kIgS1 || region == kIgC00 || region == kIgC0 ||
+         region == kIgCa;
 }
 
 // Region of (a, x) from cheap float arithmetic.
-__device__ __forceinline__ int igamma_classify(double ad, double xd, const IgPre& P) {
+// MIXED_FWD: the mixed forward's bucket kIgCa; the other kernels bucket
+// those elements by iteration count.
+__device__ __forceinline__ int igamma_classify(double ad, double xd, const IgPre& P, bool mixed_fwd = false) {
   if (!(xd >= 0.0) || !(ad > 0.0) || xd == 0.0 || isinf(xd) || isinf(ad)) return kIgSpecial;
   const float a = (float)ad, x = (float)xd;
   if (!(a > 0.0f) || !(x > 0.0f) || isinf(a) || isinf(x)) return kIgSpecial;
@@ -319,15 +380,16 @@ __device__ __forceinline__ int igamma_classify(double ad, double xd, const IgPre
   if (x < a + 1.0f) {
     // P <= D·(a+1)/(a+1-x) ~ D·a.
     if (lnd + P.la1f() + lratio < -760.0f) return kIgSat0;
-    if (a < 1.0f) return kIgSmallA;
-    return lam < 0.1f ? kIgS0 : lam < 0.35f ? kIgS1 : lam < 0.7f ? kIgS2 : kIgS3;
+    if (a < 1.0f) return lam < 0.1f ? kIgSmallA0 : kIgSmallA;
+    return lam < 0.01f ? kIgS00 : lam < 0.1f ? kIgS0 : lam < 0.35f ? kIgS1 : lam < 0.7f ? kIgS2 : kIgS3;
   }
   // Q = a D F with F <= 1/(x+1-a) <= 1.
   if (lnd + P.laf() + lratio < -760.0f) return kIgSat1;
-  return lam > 3.0f ? kIgC0 : lam > 1.5f ? kIgC1 : kIgC2;
+  if (mixed_fwd && a < 1.0f) return kIgCa;
+  return lam > 10.0f ? kIgC00 : lam > 3.0f ? kIgC0 : lam > 1.5f ? kIgC1 : kIgC2;
 }
-__device__ __forceinline__ int igamma_classify(double ad, double xd) {
-  return igamma_classify(ad, xd, IgPre{nullptr, nullptr, ad, xd});
+__device__ __forceinline__ int igamma_classify(double ad, double xd, bool mixed_fwd = false) {
+  return igamma_classify(ad, xd, IgPre{nullptr, nullptr, ad, xd}, mixed_fwd);
 }
 
 // Q(a, x) for a < 1, x < a + 1 without the 1 - P cancellation (P -> 1 as
@@ -433,65 +495,69 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
   return o;
 }
 
-// Mixed evaluation for float data: the prefactor and the ψ terms in double
-// (they carry the a·ln x cancellation), the series / continued fraction in
-// float for the light regions, everything in double for the heavy regions
-// (large a near the transition x ~ a, where the term count grows like √a and
-// float accumulation would exceed 1e-6).
-template <int ORDER, bool WANT_Q = false>
-__device__ inline IgammaOut igamma_eval_m(int region, float af, float xf, const IgPre& P) {
-  if (region == kIgSmallA) {
-    if (WANT_Q) return igamma_eval_d<ORDER, true>((double)af, (double)xf, P);
-    region = kIgS1;
-  }
-  if (!igamma_fp32_ok(region)) return igamma_eval_d<ORDER>((double)af, (double)xf, P);
+// Mixed evaluation of P or Q alone (the forward) in the light regions
+// (igamma_fp32_ok), entirely in FP32: ln D in float-float from the double
+// per-row / per-column quantities (the tables, or computed here), D =
+// exp(hi)(1 + lo), and the series or continued fraction in float.  In these
+// regions x < 0.35 (a+1) or x > 3 (a+1) (or a < 1 for the continued
+// fraction), so for a >= 10 the prefactor is always the direct form
+// a (ln x - ln a) - (x - a) - C(a).  The float continued fraction carries
+// ~1e-6 relative error in Q, which P = 1 - Q scales down by Q/P < 1 in these
+// regions; Q itself takes the FP64 continued fraction.
+template <bool WANT_Q>
+__device__ inline IgammaOut igamma_eval_mf(int region, float a, float x, const IgPre& P) {
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
-  const double a = af, x = xf;
-  const double lnD = igamma_log_prefix_d(a, x, P);
-  const double lx = P.lx();
-  double psi_a = 0.0, psi1_a = 0.0;
-  if (ORDER >= 1) psi_a = P.psi();
-  if (ORDER >= 2) psi1_a = P.psi1();
-  if (region != kIgC0) {
-    float Sf, S1f = 0.0f, S2f = 0.0f;
-    igamma_series<float, ORDER>(af, xf, Sf, S1f, S2f);
-    const double S = Sf, S1 = S1f, S2 = S2f;
-    const double D = exp(lnD);
-    o.p = D * S;
-    o.q = 1.0 - o.p;
-    if (ORDER >= 1) {
-      const double L1 = lx - (psi_a + P.ra());
-      o.pa = D * fma(L1, S, S1);
-      o.px = igamma_px_from(D, lnD, a, P);
-      if (ORDER >= 2) {
-        const double L2 = -(psi1_a - P.ra() * P.ra());
-        o.paa = D * ((L2 + L1 * L1) * S + 2.0 * L1 * S1 + S2);
-        o.pax = o.px * (lx - psi_a);
-        o.pxx = o.px * ((a - 1.0) / x - 1.0);
-      }
-    }
+  const IgFF lx = P.lxff(), lg = P.lgff();
+  IgFF lnD;
+  if (a < 10.0f) {
+    lnD = ff_add(ff_add(ff_mul_f(lx, a), IgFF{-x, 0.0f}), ff_neg(lg));
   } else {
-    float Ff, F1f = 0.0f, F2f = 0.0f;
-    igamma_cf<float, ORDER>(af, xf, Ff, F1f, F2f);
-    const double F = Ff, F1 = F1f, F2 = F2f;
-    const double lnE = lnD + P.la();
-    const double E = exp(lnE);
-    o.q = E * F;
-    o.p = 1.0 - o.q;
-    if (ORDER >= 1) {
-      const double E1 = lx - psi_a;
-      o.pa = -E * fma(E1, F, F1);
-      o.px = lnE > -700.0 ? E * P.rx() : exp(lnE - lx);  // E/x
-      if (ORDER >= 2) {
-        const double E2 = -psi1_a;
-        o.paa = -E * ((E2 + E1 * E1) * F + 2.0 * E1 * F1 + F2);
-        o.pax = o.px * E1;
-        o.pxx = o.px * ((a - 1.0) / x - 1.0);
-      }
+    const IgFF d = ff_add(lx, ff_neg(P.laff()));
+    lnD = ff_add(ff_add(ff_mul_f(d, a), ff_neg(ff_two_sum(x, -a))), ff_neg(lg));
+  }
+  if (region != kIgC0 && region != kIgC00 && region != kIgCa) {
+    float S, S1, S2;
+    igamma_series<float, 0>(a, x, S, S1, S2);
+    const float pv = ff_exp(lnD) * S;
+    o.p = pv;
+    o.q = 1.0 - (double)pv;
+  } else {
+    double F;
+    if (WANT_Q) {
+      double F1, F2;
+      igamma_cf<double, 0>((double)a, (double)x, F, F1, F2);
+    } else {
+      float f, f1, f2;
+      igamma_cf<float, 0>(a, x, f, f1, f2);
+      F = f;
     }
+    o.q = (double)ff_exp(ff_add(lnD, P.laff())) * F;  // E F, E = D a
+    o.p = 1.0 - o.q;
   }
   return o;
+}
+
+// Evaluation for float data.  P or Q alone (ORDER 0): FP32 in the light
+// regions (igamma_eval_mf), FP64 elsewhere: the heavy regions (large a near
+// the transition x ~ a, where the term count grows like √a and float
+// accumulation would exceed 1e-6) and the small-a Q.  Derivatives (ORDER >= 1)
+// are evaluated in FP64 throughout: the a-derivative of the continued
+// fraction and of the longer series loses ~1e-5 in FP32, and a kernel holding
+// both precisions' code paths measured slower than the FP64 one (instruction
+// fetch) on the 4096 x 4096 grid.
+template <int ORDER, bool WANT_Q = false>
+__device__ inline IgammaOut igamma_eval_m(int region, float af, float xf, const IgPre& P) {
+  if constexpr (ORDER >= 1) {
+    return igamma_eval_d<ORDER, WANT_Q>((double)af, (double)xf, P);
+  } else {
+    if (region == kIgSmallA || region == kIgSmallA0) {
+      if (WANT_Q) return igamma_eval_d<0, true>((double)af, (double)xf, P);
+      region = kIgS1;
+    }
+    if (!igamma_fp32_ok(region)) return igamma_eval_d<0, WANT_Q>((double)af, (double)xf, P);
+    return igamma_eval_mf<WANT_Q>(region, af, xf, P);
+  }
 }
 
 __device__ __forceinline__ IgammaOut igamma_saturated(bool upper_is_zero) {

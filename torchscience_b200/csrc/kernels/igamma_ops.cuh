@@ -41,7 +41,7 @@ struct IgammaAuxIO {
     return IgPre{A, X, (double)in[IA], (double)in[IX]};
   }
   __device__ static int classify(const T* in, const double* A = nullptr, const double* X = nullptr) {
-    return igamma_classify((double)in[IA], (double)in[IX], pre(in, A, X));
+    return igamma_classify((double)in[IA], (double)in[IX], pre(in, A, X), sizeof(T) == 4 && ORDER == 0);
   }
 };
 
