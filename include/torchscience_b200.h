@@ -185,6 +185,21 @@ TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1);
 TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1_backward);
 TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1_backward_backward);
 
+/* ---- Probability callers of the incomplete gamma ----------------------- */
+/* gamma_cumulative_distribution(x, shape, scale): kernel/probability/gamma_cumulative_distribution.h:9-13,
+ * schema torchscience.cpp:1909-1910; backward gamma_cumulative_distribution_backward.h:16-43
+ * (outputs grad_x, grad_shape, grad_scale). */
+TSB_OP_SIGNATURE(tsb_gamma_cumulative_distribution);
+TSB_OP_SIGNATURE(tsb_gamma_cumulative_distribution_backward);
+/* chi2_cumulative_distribution(x, df): chi2_cumulative_distribution.h:9-13, schema
+ * torchscience.cpp:1881-1882; backward chi2_cumulative_distribution_backward.h:31-37. */
+TSB_OP_SIGNATURE(tsb_chi2_cumulative_distribution);
+TSB_OP_SIGNATURE(tsb_chi2_cumulative_distribution_backward);
+/* poisson_cumulative_distribution(k, rate): poisson_cumulative_distribution.h:10-18, schema
+ * torchscience.cpp:1923-1924; backward poisson_cumulative_distribution_backward.h:13-29 (grad_k = 0). */
+TSB_OP_SIGNATURE(tsb_poisson_cumulative_distribution);
+TSB_OP_SIGNATURE(tsb_poisson_cumulative_distribution_backward);
+
 /* ---- Complete elliptic integrals --------------------------------------- */
 /* complete_legendre_elliptic_integral_k(m): complete_legendre_elliptic_integral_k.h:29-33,
  * schema torchscience.cpp:1015-1017; backward ..._k_backward.h:24-53,

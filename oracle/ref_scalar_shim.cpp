@@ -15,6 +15,12 @@
 #include <cstring>
 #include <tuple>
 
+#include "kernel/probability/chi2_cumulative_distribution.h"
+#include "kernel/probability/chi2_cumulative_distribution_backward.h"
+#include "kernel/probability/gamma_cumulative_distribution.h"
+#include "kernel/probability/gamma_cumulative_distribution_backward.h"
+#include "kernel/probability/poisson_cumulative_distribution.h"
+#include "kernel/probability/poisson_cumulative_distribution_backward.h"
 #include "kernel/special_functions/bessel_j.h"
 #include "kernel/special_functions/bessel_j_0.h"
 #include "kernel/special_functions/bessel_j_0_backward.h"
@@ -59,6 +65,7 @@
 #include "kernel/special_functions/trigamma_backward_backward.h"
 
 namespace sf = torchscience::kernel::special_functions;
+namespace pr = torchscience::kernel::probability;
 
 namespace {
 
@@ -142,6 +149,21 @@ static int eval_typed(const char* name, int pass, const void* const* in, void* c
   BINARY(bessel_y)
   BINARY(modified_bessel_i)
   BINARY(modified_bessel_k)
+  if (std::strcmp(name, "gamma_cumulative_distribution") == 0) {
+    if (pass == 0) LOOP(pr::gamma_cumulative_distribution(ARG(0), ARG(1), ARG(2)));
+    if (pass == 1) LOOP(pr::gamma_cumulative_distribution_backward(ARG(0), ARG(1), ARG(2), ARG(3)));
+    return -1;
+  }
+  if (std::strcmp(name, "chi2_cumulative_distribution") == 0) {
+    if (pass == 0) LOOP(pr::chi2_cumulative_distribution(ARG(0), ARG(1)));
+    if (pass == 1) LOOP(pr::chi2_cumulative_distribution_backward(ARG(0), ARG(1), ARG(2)));
+    return -1;
+  }
+  if (std::strcmp(name, "poisson_cumulative_distribution") == 0) {
+    if (pass == 0) LOOP(pr::poisson_cumulative_distribution(ARG(0), ARG(1)));
+    if (pass == 1) LOOP(pr::poisson_cumulative_distribution_backward(ARG(0), ARG(1), ARG(2)));
+    return -1;
+  }
   if (std::strcmp(name, "hypergeometric_2_f_1") == 0) {
     if (pass == 0) LOOP(sf::hypergeometric_2_f_1(ARG(0), ARG(1), ARG(2), ARG(3)));
     if (pass == 1) LOOP(sf::hypergeometric_2_f_1_backward(ARG(0), ARG(1), ARG(2), ARG(3), ARG(4)));

@@ -247,8 +247,67 @@ def hyp2f1():
     np.savez_compressed(OUT / "hyp2f1.npz", **d)
 
 
+def _dP_da(a, x):
+    """∂P/∂a by mpmath, as -∂Q/∂a where x > a (P is then close to 1 and its
+    difference quotient would lose the digits)."""
+    a, x = mp.mpf(a), mp.mpf(x)
+    if x > a:
+        return -float(mp.diff(lambda t: mp.gammainc(t, x, mp.inf, regularized=True), a))
+    return float(mp.diff(lambda t: mp.gammainc(t, 0, x, regularized=True), a))
+
+
+def probability():
+    """Gamma / chi-squared / Poisson CDF fixtures: seeded inputs, scipy values
+    and densities, mpmath a-derivatives on a subsample, the reference's outputs
+    and backward outputs, and its boundary cases (x <= 0, k < 0, NaN)."""
+    import scipy.stats as st
+
+    rng = np.random.default_rng(5)
+    n = 3000
+    d = {}
+    # gamma
+    x, sh, sc = lu(rng, 1e-3, 1e3, n), lu(rng, 0.1, 100.0, n), lu(rng, 0.1, 10.0, n)
+    x[:20] = [0.0, -1.0, np.nan] + [1.0] * 17
+    g = rng.standard_normal(n)
+    d["gamma_x"], d["gamma_shape"], d["gamma_scale"], d["gamma_g"] = x, sh, sc, g
+    with np.errstate(invalid="ignore"):
+        d["gamma_truth"] = np.where(x > 0, st.gamma.cdf(x, sh, scale=sc), np.where(np.isnan(x), np.nan, 0.0))
+        d["gamma_truth_pdf"] = np.where(x > 0, st.gamma.pdf(x, sh, scale=sc), np.where(np.isnan(x), np.nan, 0.0))
+    d["gamma_ref"] = ref("gamma_cumulative_distribution", 0, x, sh, sc)[0]
+    d["gamma_ref_grad"] = np.stack(ref("gamma_cumulative_distribution", 1, g, x, sh, sc), axis=1)
+    idx = np.arange(20, 220)
+    d["gamma_dshape_idx"] = idx
+    d["gamma_truth_dshape"] = np.array([_dP_da(sh[i], mp.mpf(x[i]) / mp.mpf(sc[i])) for i in idx])
+    # chi2
+    x2, df = lu(rng, 1e-3, 1e3, n), lu(rng, 0.2, 200.0, n)
+    x2[:3] = [0.0, -2.0, np.nan]
+    g2 = rng.standard_normal(n)
+    d["chi2_x"], d["chi2_df"], d["chi2_g"] = x2, df, g2
+    with np.errstate(invalid="ignore"):
+        d["chi2_truth"] = np.where(x2 > 0, st.chi2.cdf(x2, df), np.where(np.isnan(x2), np.nan, 0.0))
+        d["chi2_truth_pdf"] = np.where(x2 > 0, st.chi2.pdf(x2, df), np.where(np.isnan(x2), np.nan, 0.0))
+    d["chi2_ref"] = ref("chi2_cumulative_distribution", 0, x2, df)[0]
+    d["chi2_ref_grad"] = np.stack(ref("chi2_cumulative_distribution", 1, g2, x2, df), axis=1)
+    idx2 = np.arange(3, 203)
+    d["chi2_ddf_idx"] = idx2
+    d["chi2_truth_ddf"] = np.array([0.5 * _dP_da(df[i] / 2, mp.mpf(x2[i]) / 2) for i in idx2])
+    # poisson
+    k = np.concatenate([rng.integers(0, 120, n - 6).astype(float) + np.where(rng.random(n - 6) < 0.2, 0.5, 0.0),
+                        [-1.0, -0.5, 0.0, 3.7, np.nan, 10.0]])
+    rate = np.concatenate([lu(rng, 1e-2, 100.0, n - 6), [1.0, 1.0, 2.5, 2.5, 1.0, np.nan]])
+    g3 = rng.standard_normal(n)
+    d["poisson_k"], d["poisson_rate"], d["poisson_g"] = k, rate, g3
+    kf = np.floor(k)
+    with np.errstate(invalid="ignore"):
+        d["poisson_truth"] = np.where(kf >= 0, st.poisson.cdf(kf, rate), np.where(np.isnan(kf), np.nan, 0.0))
+        d["poisson_truth_drate"] = np.where(kf >= 0, -st.poisson.pmf(kf, rate), np.where(np.isnan(kf), np.nan, 0.0))
+    d["poisson_ref"] = ref("poisson_cumulative_distribution", 0, k, rate)[0]
+    d["poisson_ref_grad"] = np.stack(ref("poisson_cumulative_distribution", 1, g3, k, rate), axis=1)
+    np.savez_compressed(OUT / "probability.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "hyp2f1"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "hyp2f1", "probability"]
     for w in which:
         globals()[w]()
         print("wrote", w)

@@ -30,6 +30,13 @@ REFERENCE_SCHEMAS = [
     "hypergeometric_2_f_1_backward(Tensor grad_output, Tensor a, Tensor b, Tensor c, Tensor z) -> (Tensor, Tensor, Tensor, Tensor)",
     "complete_legendre_elliptic_integral_k(Tensor m) -> Tensor",
     "complete_legendre_elliptic_integral_e_backward_backward(Tensor gg_m, Tensor grad_output, Tensor m) -> (Tensor, Tensor)",
+    # probability callers (torchscience.cpp:1881-1924)
+    "chi2_cumulative_distribution(Tensor x, Tensor df) -> Tensor",
+    "chi2_cumulative_distribution_backward(Tensor grad, Tensor x, Tensor df) -> (Tensor, Tensor)",
+    "gamma_cumulative_distribution(Tensor x, Tensor shape, Tensor scale) -> Tensor",
+    "gamma_cumulative_distribution_backward(Tensor grad, Tensor x, Tensor shape, Tensor scale) -> (Tensor, Tensor, Tensor)",
+    "poisson_cumulative_distribution(Tensor k, Tensor rate) -> Tensor",
+    "poisson_cumulative_distribution_backward(Tensor grad, Tensor k, Tensor rate) -> (Tensor, Tensor)",
 ]
 
 
@@ -94,3 +101,17 @@ def test_precision_mode_api():
     assert tsb.get_precision_mode() == "mixed"
     with pytest.raises(ValueError):
         tsb.set_precision_mode("fp16")
+
+
+def test_probability_meta_shapes_and_reduced_gradients():
+    from torchscience_b200 import probability as pb
+
+    x = meta(5, 1, rg=True)
+    sh = meta(1, 3, rg=True)
+    sc = meta(1, rg=True)
+    y = pb.gamma_cumulative_distribution(x, sh, sc)
+    assert y.shape == (5, 3) and y.device.type == "meta"
+    gx, gs, gc = torch.autograd.grad(y.sum(), (x, sh, sc))
+    assert gx.shape == x.shape and gs.shape == sh.shape and gc.shape == sc.shape
+    assert pb.chi2_cumulative_distribution(meta(4, dtype=torch.float64), 3.0).dtype == torch.float64
+    assert pb.poisson_cumulative_distribution(meta(2, 1), meta(6)).shape == (2, 6)

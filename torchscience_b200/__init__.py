@@ -25,10 +25,11 @@ if not (_os.path.exists(KERNEL_LIBRARY) and _os.path.exists(OPS_LIBRARY)):
 
 _torch.ops.load_library(OPS_LIBRARY)
 
-from . import special_functions  # noqa: E402
+from . import probability, special_functions  # noqa: E402
 from ._precision import get_precision_mode, precision, set_precision_mode  # noqa: E402
 
 __all__ = [
+    "probability",
     "special_functions",
     "set_precision_mode",
     "get_precision_mode",

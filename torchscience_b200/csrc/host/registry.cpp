@@ -437,6 +437,188 @@ TORCH_LIBRARY_IMPL(torchscience, CPU, m) {
 TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_autograd); }
 TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_autocast); }
 
+// ------------------------------------------- probability callers of P and Q
+// gamma / chi2 / poisson cumulative distributions (torchscience.cpp:1881-1924).
+// As in the reference (autograd/probability/*.h, cpu/probability/*.h), the
+// backward ops return gradients already reduced to the inputs' shapes and
+// have no double backward.
+namespace tsbh::prob {
+using T2 = std::tuple<at::Tensor, at::Tensor>;
+using T3 = std::tuple<at::Tensor, at::Tensor, at::Tensor>;
+
+inline std::vector<at::Tensor> meta_grads(at::TensorList ins) {
+  at::ScalarType dt = ins[0].scalar_type();
+  for (const auto& t : ins) dt = at::promote_types(dt, t.scalar_type());
+  std::vector<at::Tensor> r;
+  for (const auto& t : ins) r.push_back(at::empty(t.sizes(), t.options().dtype(dt).device(at::kMeta)));
+  return r;
+}
+inline std::vector<at::Tensor> reduced_all(OpFn fn, const char* name, const at::Tensor& g, at::TensorList ins) {
+  return run_reduced_backward(fn, name, g, ins, std::vector<bool>(ins.size(), true));
+}
+
+at::Tensor chi2_cuda(const at::Tensor& x, const at::Tensor& df) {
+  return run_pointwise(tsb_chi2_cumulative_distribution, "chi2_cumulative_distribution", {x, df}, 1)[0];
+}
+T2 chi2_backward_cuda(const at::Tensor& g, const at::Tensor& x, const at::Tensor& df) {
+  auto r = reduced_all(tsb_chi2_cumulative_distribution_backward, "chi2_cumulative_distribution_backward", g, {x, df});
+  return {r[0], r[1]};
+}
+at::Tensor gamma_cdf_cuda(const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
+  return run_pointwise(tsb_gamma_cumulative_distribution, "gamma_cumulative_distribution", {x, shape, scale}, 1)[0];
+}
+T3 gamma_cdf_backward_cuda(const at::Tensor& g, const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
+  auto r = reduced_all(tsb_gamma_cumulative_distribution_backward, "gamma_cumulative_distribution_backward", g,
+                       {x, shape, scale});
+  return {r[0], r[1], r[2]};
+}
+at::Tensor poisson_cuda(const at::Tensor& k, const at::Tensor& rate) {
+  return run_pointwise(tsb_poisson_cumulative_distribution, "poisson_cumulative_distribution", {k, rate}, 1)[0];
+}
+T2 poisson_backward_cuda(const at::Tensor& g, const at::Tensor& k, const at::Tensor& rate) {
+  auto r = reduced_all(tsb_poisson_cumulative_distribution_backward, "poisson_cumulative_distribution_backward", g,
+                       {k, rate});
+  return {r[0], r[1]};
+}
+
+at::Tensor chi2_meta(const at::Tensor& x, const at::Tensor& df) {
+  return meta_pointwise("chi2_cumulative_distribution", {x, df}, 1)[0];
+}
+T2 chi2_backward_meta(const at::Tensor& g, const at::Tensor& x, const at::Tensor& df) {
+  auto r = meta_grads({x, df});
+  return {r[0], r[1]};
+}
+at::Tensor gamma_cdf_meta(const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
+  return meta_pointwise("gamma_cumulative_distribution", {x, shape, scale}, 1)[0];
+}
+T3 gamma_cdf_backward_meta(const at::Tensor& g, const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
+  auto r = meta_grads({x, shape, scale});
+  return {r[0], r[1], r[2]};
+}
+at::Tensor poisson_meta(const at::Tensor& k, const at::Tensor& rate) {
+  return meta_pointwise("poisson_cumulative_distribution", {k, rate}, 1)[0];
+}
+T2 poisson_backward_meta(const at::Tensor& g, const at::Tensor& k, const at::Tensor& rate) {
+  auto r = meta_grads({k, rate});
+  return {r[0], r[1]};
+}
+
+at::Tensor chi2_cpu(const at::Tensor&, const at::Tensor&) { cpu_not_supported("chi2_cumulative_distribution"); }
+T2 chi2_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&) {
+  cpu_not_supported("chi2_cumulative_distribution_backward");
+}
+at::Tensor gamma_cdf_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&) {
+  cpu_not_supported("gamma_cumulative_distribution");
+}
+T3 gamma_cdf_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&) {
+  cpu_not_supported("gamma_cumulative_distribution_backward");
+}
+at::Tensor poisson_cpu(const at::Tensor&, const at::Tensor&) { cpu_not_supported("poisson_cumulative_distribution"); }
+T2 poisson_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&) {
+  cpu_not_supported("poisson_cumulative_distribution_backward");
+}
+
+template <typename Sig>
+inline auto op(const char* name) {
+  return c10::Dispatcher::singleton().findSchemaOrThrow(name, "").typed<Sig>();
+}
+
+class Chi2Cdf : public torch::autograd::Function<Chi2Cdf> {
+ public:
+  static at::Tensor forward(AutogradContext* ctx, const at::Tensor& x, const at::Tensor& df) {
+    ctx->save_for_backward({x, df});
+    at::AutoDispatchBelowAutograd guard;
+    static auto f = op<at::Tensor(const at::Tensor&, const at::Tensor&)>("torchscience::chi2_cumulative_distribution");
+    return f.call(x, df);
+  }
+  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
+    auto s = ctx->get_saved_variables();
+    if (!go[0].defined()) return {at::Tensor(), at::Tensor()};
+    at::AutoDispatchBelowAutograd guard;
+    static auto b = op<T2(const at::Tensor&, const at::Tensor&, const at::Tensor&)>(
+        "torchscience::chi2_cumulative_distribution_backward");
+    auto [gx, gdf] = b.call(go[0], s[0], s[1]);
+    return {gx, gdf};
+  }
+};
+class GammaCdf : public torch::autograd::Function<GammaCdf> {
+ public:
+  static at::Tensor forward(AutogradContext* ctx, const at::Tensor& x, const at::Tensor& shape,
+                            const at::Tensor& scale) {
+    ctx->save_for_backward({x, shape, scale});
+    at::AutoDispatchBelowAutograd guard;
+    static auto f = op<at::Tensor(const at::Tensor&, const at::Tensor&, const at::Tensor&)>(
+        "torchscience::gamma_cumulative_distribution");
+    return f.call(x, shape, scale);
+  }
+  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
+    auto s = ctx->get_saved_variables();
+    if (!go[0].defined()) return {at::Tensor(), at::Tensor(), at::Tensor()};
+    at::AutoDispatchBelowAutograd guard;
+    static auto b = op<T3(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&)>(
+        "torchscience::gamma_cumulative_distribution_backward");
+    auto [gx, gs, gc] = b.call(go[0], s[0], s[1], s[2]);
+    return {gx, gs, gc};
+  }
+};
+class PoissonCdf : public torch::autograd::Function<PoissonCdf> {
+ public:
+  static at::Tensor forward(AutogradContext* ctx, const at::Tensor& k, const at::Tensor& rate) {
+    ctx->save_for_backward({k, rate});
+    at::AutoDispatchBelowAutograd guard;
+    static auto f =
+        op<at::Tensor(const at::Tensor&, const at::Tensor&)>("torchscience::poisson_cumulative_distribution");
+    return f.call(k, rate);
+  }
+  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
+    auto s = ctx->get_saved_variables();
+    if (!go[0].defined()) return {at::Tensor(), at::Tensor()};
+    at::AutoDispatchBelowAutograd guard;
+    static auto b = op<T2(const at::Tensor&, const at::Tensor&, const at::Tensor&)>(
+        "torchscience::poisson_cumulative_distribution_backward");
+    auto [gk, gr] = b.call(go[0], s[0], s[1]);
+    return {gk, gr};
+  }
+};
+
+at::Tensor chi2_autograd(const at::Tensor& x, const at::Tensor& df) { return Chi2Cdf::apply(x, df); }
+at::Tensor gamma_cdf_autograd(const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
+  return GammaCdf::apply(x, shape, scale);
+}
+at::Tensor poisson_autograd(const at::Tensor& k, const at::Tensor& rate) { return PoissonCdf::apply(k, rate); }
+}  // namespace tsbh::prob
+
+TORCH_LIBRARY_FRAGMENT(torchscience, m) { TSB_DEFINE_PROBABILITY_SCHEMAS(m) }
+TORCH_LIBRARY_IMPL(torchscience, CUDA, m) {
+  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_cuda);
+  m.impl("chi2_cumulative_distribution_backward", tsbh::prob::chi2_backward_cuda);
+  m.impl("gamma_cumulative_distribution", tsbh::prob::gamma_cdf_cuda);
+  m.impl("gamma_cumulative_distribution_backward", tsbh::prob::gamma_cdf_backward_cuda);
+  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_cuda);
+  m.impl("poisson_cumulative_distribution_backward", tsbh::prob::poisson_backward_cuda);
+}
+TORCH_LIBRARY_IMPL(torchscience, Meta, m) {
+  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_meta);
+  m.impl("chi2_cumulative_distribution_backward", tsbh::prob::chi2_backward_meta);
+  m.impl("gamma_cumulative_distribution", tsbh::prob::gamma_cdf_meta);
+  m.impl("gamma_cumulative_distribution_backward", tsbh::prob::gamma_cdf_backward_meta);
+  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_meta);
+  m.impl("poisson_cumulative_distribution_backward", tsbh::prob::poisson_backward_meta);
+}
+TORCH_LIBRARY_IMPL(torchscience, CPU, m) {
+  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_cpu);
+  m.impl("chi2_cumulative_distribution_backward", tsbh::prob::chi2_backward_cpu);
+  m.impl("gamma_cumulative_distribution", tsbh::prob::gamma_cdf_cpu);
+  m.impl("gamma_cumulative_distribution_backward", tsbh::prob::gamma_cdf_backward_cpu);
+  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_cpu);
+  m.impl("poisson_cumulative_distribution_backward", tsbh::prob::poisson_backward_cpu);
+}
+TORCH_LIBRARY_IMPL(torchscience, Autograd, m) {
+  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_autograd);
+  m.impl("gamma_cumulative_distribution", tsbh::prob::gamma_cdf_autograd);
+  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_autograd);
+}
+
 // Library-level controls (not part of the reference's namespace).
 namespace tsbh {
 int64_t set_precision_mode(int64_t mode) {

@@ -83,3 +83,15 @@
   (m).def(                                                                                                           \
       "complete_legendre_elliptic_integral_e_backward_backward(Tensor gg_m, Tensor grad_output, Tensor m) -> "       \
       "(Tensor, Tensor)");
+
+// Schemas of the probability callers of the incomplete gamma (torchscience.cpp:1881-1882, 1909-1910,
+// 1923-1924), registered by this package only.
+#define TSB_DEFINE_PROBABILITY_SCHEMAS(m)                                                                             \
+  (m).def("chi2_cumulative_distribution(Tensor x, Tensor df) -> Tensor");                                            \
+  (m).def("chi2_cumulative_distribution_backward(Tensor grad, Tensor x, Tensor df) -> (Tensor, Tensor)");            \
+  (m).def("gamma_cumulative_distribution(Tensor x, Tensor shape, Tensor scale) -> Tensor");                          \
+  (m).def(                                                                                                           \
+      "gamma_cumulative_distribution_backward(Tensor grad, Tensor x, Tensor shape, Tensor scale) -> (Tensor, Tensor, " \
+      "Tensor)");                                                                                                    \
+  (m).def("poisson_cumulative_distribution(Tensor k, Tensor rate) -> Tensor");                                       \
+  (m).def("poisson_cumulative_distribution_backward(Tensor grad, Tensor k, Tensor rate) -> (Tensor, Tensor)");
