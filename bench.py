@@ -585,6 +585,31 @@ def secondary_arm(args):
                 row["mixed_max_rel_err_vs_fp64"] = _max_rel(fn(nu32, x32), fn(nu32.double(), x32.double()))
             row["mixed_speedup_fwd_bwd"] = row["mixed_fwd_bwd_gelem_s"] / row["fp64_fwd_bwd_gelem_s"]
             res[name] = row
+        del nu64, x64, nu32, x32, g32
+        # 2^20 points within relative 1e-6 of the first 100 zeros of J0 (ν = 0) and J1 (ν = 1)
+        import numpy as np
+        import scipy.special as sp
+
+        nz = 1 << 20
+        zeros = torch.tensor(np.concatenate([sp.jn_zeros(0, 100), sp.jn_zeros(1, 100)]), device=dev)
+        orders = torch.cat([torch.zeros(100, device=dev, dtype=torch.float64),
+                            torch.ones(100, device=dev, dtype=torch.float64)])
+        pick = torch.randint(0, 200, (nz,), generator=gen, device=dev)
+        nuz, xz = orders[pick], zeros[pick] * (1.0 + U(nz, -1e-6, 1e-6))
+        gz = torch.randn(nz, generator=gen, device=dev, dtype=torch.float64)
+        row = {}
+        for tag, dt in (("mixed", torch.float32), ("fp64", torch.float64)):
+            nu, x, g = nuz.to(dt), xz.to(dt), gz.to(dt)
+            xr = x.clone().requires_grad_(True)
+
+            def fbz():
+                y = sf.bessel_j(nu, xr)
+                torch.autograd.grad(y, xr, g)
+
+            with torch.no_grad():
+                row[f"{tag}_fwd_gelem_s"] = _rate(lambda: sf.bessel_j(nu, x), nz, S, W, flush)
+            row[f"{tag}_fwd_bwd_gelem_s"] = _rate(fbz, nz, S, W, flush)
+        res["bessel_j_near_zeros_of_j0_j1_2^20"] = row
     elif args.workload == "c4":
         n = 1 << 24
         desc = ("hypergeometric_2_f_1, a, b ~ U(-10, 10), c ~ U(-10, 10) (|c - round c| >= 1e-3 for c <= 0), "

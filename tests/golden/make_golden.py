@@ -179,6 +179,25 @@ def bessel():
     np.savez_compressed(OUT / "bessel.npz", **d)
 
 
+def bessel01():
+    """J0 and J1 on the order-0/1 path: uniform and log-uniform arguments, both
+    signs, and points within relative 1e-13..1e-3 of the zeros of J0 and J1
+    below 60, with mpmath values of J0, J1 and J0'', and the reference's
+    bessel_j_0 forward and backward."""
+    rng = np.random.default_rng(8)
+    z0, z1 = sp.jn_zeros(0, 19), sp.jn_zeros(1, 19)
+    zs = np.concatenate([z0, z1])
+    near = np.repeat(zs, 8) * (1.0 + rng.choice([-1.0, 1.0], zs.size * 8) * lu(rng, 1e-13, 1e-3, zs.size * 8))
+    x = np.concatenate([rng.uniform(0.0, 60.0, 2000), -rng.uniform(0.0, 60.0, 300), lu(rng, 1e-8, 1e6, 600), near])
+    d = {"x": x, "g": rng.standard_normal(x.size)}
+    d["truth_j0"] = np.array([float(mp.besselj(0, mp.mpf(v))) for v in x])
+    d["truth_j1"] = np.array([float(mp.besselj(1, mp.mpf(v))) for v in x])
+    d["truth_j0pp"] = np.array([float(mp.besselj(0, mp.mpf(v), derivative=2)) for v in x])
+    d["ref_j0"] = ref("bessel_j_0", 0, x)[0]
+    d["ref_j0_grad"] = ref("bessel_j_0", 1, d["g"], x)[0]
+    np.savez_compressed(OUT / "bessel01.npz", **d)
+
+
 def hyp2f1():
     """2F1 fixtures: the reference's known answers, its scipy grid, a seeded
     sample of the benchmark distribution (a, b, c ~ U(-10, 10), c rejected
@@ -307,7 +326,7 @@ def probability():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "hyp2f1", "probability"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability"]
     for w in which:
         globals()[w]()
         print("wrote", w)

@@ -28,6 +28,7 @@
 
 #include <math_constants.h>
 
+#include "bessel01_math.cuh"
 #include "fits.cuh"
 #include "gamma_math.cuh"
 

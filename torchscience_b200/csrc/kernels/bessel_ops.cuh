@@ -20,13 +20,18 @@
 namespace tsb {
 
 enum BesselKind : int { kBJ = 0, kBY = 1, kBI = 2, kBK = 3 };
-enum BesselRegion : int { kBsSpecial = 0, kBsSeries = 1, kBsMid = 2, kBsLarge = 3, kBsRegions = 4 };
+enum BesselRegion : int { kBsSpecial = 0, kBsSeries = 1, kBsMid = 2, kBsLarge = 3, kBsJ01 = 4, kBsRegions = 5 };
+
+// J at order 0 or ±1 with finite, non-zero x: the dedicated J0/J1 path.
+__device__ __forceinline__ bool bessel_j01_order(double nu) { return nu == 0.0 || fabs(nu) == 1.0; }
 
 // Evaluation region (also the unit of compaction).  Mixed kernels run
-// kBsSeries (x < 2, order >= 0 or integer) in FP32 and the others in FP64.
+// kBsSeries (x < 2, order >= 0 or integer) in FP32 and the others in FP64;
+// kBsJ01 is J at order 0, ±1.
 template <int KIND>
 __device__ __forceinline__ int bessel_classify(double nu, double x) {
   if (isnan(nu) || isnan(x) || isinf(nu) || isinf(x) || x == 0.0) return kBsSpecial;
+  if (KIND == kBJ && bessel_j01_order(nu)) return kBsJ01;
   if ((KIND == kBY || KIND == kBK) && x < 0.0) return kBsSpecial;
   const double ax = fabs(x), an = fabs(nu);
   if (ax < 2.0) return (nu >= 0.0 || an == floor(an)) ? kBsSeries : kBsMid;
@@ -72,6 +77,12 @@ __device__ inline BV<T> bessel_eval(T nu, T x) {
     if (!is_int) return {nan, nan};
     const T s = odd_integer(an) ? T(-1) : T(1);
     return {s * inf, -s * inf};
+  }
+  if (KIND == kBJ && bessel_j01_order((double)nu)) {  // J0' = -J1, J1' = J0 - J1/x, J_{-1} = -J_1
+    const J01 b = bessel_j01_call((double)x);
+    if (nu == T(0)) return {(T)b.j0, (T)(-b.j1)};
+    const double v = b.j1, d = b.j0 - b.j1 / (double)x;
+    return nu > T(0) ? BV<T>{(T)v, (T)d} : BV<T>{(T)(-v), (T)(-d)};
   }
   const T ax = fabs(x);
   T v, d;
@@ -231,36 +242,60 @@ struct BesselBwdBwd {
   }
 };
 
-// J_0 (bessel_j_0): the same evaluator at order 0.
+// J_0 (bessel_j_0): the order-0/1 path with no region split (every finite
+// argument costs about the same); J0(0) = 1, J0(±inf) = 0 as in the
+// reference (bessel_j_0.h:91-129).  Float data is evaluated in FP64 and
+// rounded once.
 template <typename T_>
 struct BesselJ0Fwd {
   using T = T_;
-  static constexpr int NIN = 1, NOUT = 1, R = kBsRegions;
+  static constexpr int NIN = 1, NOUT = 1, R = 1;
   static constexpr bool REDUCE = false;
-  __device__ static int classify(const T* in) { return bessel_classify<kBJ>(0.0, (double)in[0]); }
-  __device__ static void eval(int r, const T* in, T* out, uint32_t) { out[0] = bessel_value<T, kBJ>(r, T(0), in[0]).v; }
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double x = in[0];
+    double v;
+    if (isnan(x)) v = x;
+    else if (isinf(x)) v = 0.0;
+    else if (x == 0.0) v = 1.0;
+    else v = bessel_j01<true, false>(x).j0;
+    out[0] = (T)v;
+  }
 };
 template <typename T_>
 struct BesselJ0Bwd {  // in = {grad, z}: grad * J0'(z) = -grad * J1(z)
   using T = T_;
-  static constexpr int NIN = 2, NOUT = 1, R = kBsRegions;
+  static constexpr int NIN = 2, NOUT = 1, R = 1;
   static constexpr bool REDUCE = false;
-  __device__ static int classify(const T* in) { return bessel_classify<kBJ>(0.0, (double)in[1]); }
-  __device__ static void eval(int r, const T* in, T* out, uint32_t) {
-    out[0] = in[0] * bessel_value<T, kBJ>(r, T(0), in[1]).d;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double g = in[0], x = in[1];
+    double d;
+    if (isnan(x)) d = x;
+    else if (isinf(x)) d = 0.0;
+    else d = -bessel_j01<false, true>(x).j1;
+    out[0] = (T)(g * d);
   }
 };
 template <typename T_>
-struct BesselJ0BwdBwd {  // in = {gg, grad, z}: {gg·J0'(z), gg·grad·J0''(z)}
+struct BesselJ0BwdBwd {  // in = {gg, grad, z}: {gg·J0'(z), gg·grad·J0''(z)}, J0'' = J1/z - J0
   using T = T_;
-  static constexpr int NIN = 3, NOUT = 2, R = kBsRegions;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
   static constexpr bool REDUCE = true;
-  __device__ static int classify(const T* in) { return bessel_classify<kBJ>(0.0, (double)in[2]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     const double gg = in[0], g = in[1], x = in[2];
-    const BV<double> b = bessel_eval<double, kBJ>(0.0, x);
-    const double d2 = x == 0.0 ? -0.5 : bessel_d2<double, kBJ>(0.0, x, b);
-    out[0] = (T)(gg * b.d);
+    double d1, d2;
+    if (isnan(x)) {
+      d1 = d2 = x;
+    } else if (isinf(x)) {
+      d1 = d2 = 0.0;
+    } else if (x == 0.0) {
+      d1 = 0.0;
+      d2 = -0.5;
+    } else {
+      const J01 b = bessel_j01<true, true, TSB_B01_UNROLL>(x);
+      d1 = -b.j1;
+      d2 = b.j1 / x - b.j0;
+    }
+    out[0] = (T)(gg * d1);
     out[1] = (T)(gg * g * d2);
   }
 };
