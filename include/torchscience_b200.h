@@ -199,6 +199,20 @@ TSB_OP_SIGNATURE(tsb_chi2_cumulative_distribution_backward);
  * torchscience.cpp:1923-1924; backward poisson_cumulative_distribution_backward.h:13-29 (grad_k = 0). */
 TSB_OP_SIGNATURE(tsb_poisson_cumulative_distribution);
 TSB_OP_SIGNATURE(tsb_poisson_cumulative_distribution_backward);
+/* chi2_survival(x, df) = Q(df/2, x/2), 1 for x <= 0: kernel/probability/chi2_survival.h:9-13, schema
+ * torchscience.cpp:1887-1888; backward chi2_survival_backward.h:11-17 (the negated CDF gradients). */
+TSB_OP_SIGNATURE(tsb_chi2_survival);
+TSB_OP_SIGNATURE(tsb_chi2_survival_backward);
+/* gamma_probability_density(x, shape, scale): gamma_probability_density.h:9-16, schema
+ * torchscience.cpp:1911-1912; backward gamma_probability_density_backward.h:17-40
+ * (outputs grad_x, grad_shape, grad_scale; 0 for x <= 0). */
+TSB_OP_SIGNATURE(tsb_gamma_probability_density);
+TSB_OP_SIGNATURE(tsb_gamma_probability_density_backward);
+/* chi2_probability_density(x, df): chi2_probability_density.h:10-21 (x = 0: inf for df < 2, 1/2 for
+ * df = 2, else 0), schema torchscience.cpp:1883-1884; backward chi2_probability_density_backward.h:11-40
+ * (outputs grad_x, grad_df; 0 for x <= 0). */
+TSB_OP_SIGNATURE(tsb_chi2_probability_density);
+TSB_OP_SIGNATURE(tsb_chi2_probability_density_backward);
 
 /* ---- Complete elliptic integrals --------------------------------------- */
 /* complete_legendre_elliptic_integral_k(m): complete_legendre_elliptic_integral_k.h:29-33,

@@ -21,6 +21,12 @@
 #include "kernel/probability/gamma_cumulative_distribution_backward.h"
 #include "kernel/probability/poisson_cumulative_distribution.h"
 #include "kernel/probability/poisson_cumulative_distribution_backward.h"
+#include "kernel/probability/chi2_survival.h"
+#include "kernel/probability/chi2_survival_backward.h"
+#include "kernel/probability/gamma_probability_density.h"
+#include "kernel/probability/gamma_probability_density_backward.h"
+#include "kernel/probability/chi2_probability_density.h"
+#include "kernel/probability/chi2_probability_density_backward.h"
 #include "kernel/special_functions/bessel_j.h"
 #include "kernel/special_functions/bessel_j_0.h"
 #include "kernel/special_functions/bessel_j_0_backward.h"
@@ -162,6 +168,21 @@ static int eval_typed(const char* name, int pass, const void* const* in, void* c
   if (std::strcmp(name, "poisson_cumulative_distribution") == 0) {
     if (pass == 0) LOOP(pr::poisson_cumulative_distribution(ARG(0), ARG(1)));
     if (pass == 1) LOOP(pr::poisson_cumulative_distribution_backward(ARG(0), ARG(1), ARG(2)));
+    return -1;
+  }
+  if (std::strcmp(name, "chi2_survival") == 0) {
+    if (pass == 0) LOOP(pr::chi2_survival(ARG(0), ARG(1)));
+    if (pass == 1) LOOP(pr::chi2_survival_backward(ARG(0), ARG(1), ARG(2)));
+    return -1;
+  }
+  if (std::strcmp(name, "gamma_probability_density") == 0) {
+    if (pass == 0) LOOP(pr::gamma_probability_density(ARG(0), ARG(1), ARG(2)));
+    if (pass == 1) LOOP(pr::gamma_probability_density_backward(ARG(0), ARG(1), ARG(2), ARG(3)));
+    return -1;
+  }
+  if (std::strcmp(name, "chi2_probability_density") == 0) {
+    if (pass == 0) LOOP(pr::chi2_probability_density(ARG(0), ARG(1)));
+    if (pass == 1) LOOP(pr::chi2_probability_density_backward(ARG(0), ARG(1), ARG(2)));
     return -1;
   }
   if (std::strcmp(name, "hypergeometric_2_f_1") == 0) {

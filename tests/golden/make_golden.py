@@ -325,8 +325,85 @@ def probability():
     np.savez_compressed(OUT / "probability.npz", **d)
 
 
+def probability_density():
+    """Gamma and chi-squared densities with their gradients, and the chi-squared
+    survival function: seeded inputs from the CDF fixtures' distributions,
+    mpmath values (40 digits) of the density, its derivatives in x, shape
+    (df) and scale, and of Q and its df-derivative on a subsample; the
+    reference's outputs and backward outputs; boundary cases (x <= 0, NaN,
+    the χ² density at x = 0 for df below, at and above 2)."""
+    rng = np.random.default_rng(9)
+    n = 2000
+    d = {}
+
+    def gpdf(x, a, s):
+        x, a, s = mp.mpf(x), mp.mpf(a), mp.mpf(s)
+        return mp.exp((a - 1) * mp.log(x) - x / s - a * mp.log(s) - mp.loggamma(a))
+
+    # gamma density
+    x, sh, sc = lu(rng, 1e-3, 1e3, n), lu(rng, 0.1, 100.0, n), lu(rng, 0.1, 10.0, n)
+    x[:3] = [0.0, -1.0, np.nan]
+    g = rng.standard_normal(n)
+    d["gamma_x"], d["gamma_shape"], d["gamma_scale"], d["gamma_g"] = x, sh, sc, g
+    t = np.zeros((n, 4))
+    for i in range(n):
+        if not x[i] > 0:
+            t[i] = [np.nan if np.isnan(x[i]) else 0.0] + [0.0] * 3
+            continue
+        f = gpdf(x[i], sh[i], sc[i])
+        X, a, s = mp.mpf(x[i]), mp.mpf(sh[i]), mp.mpf(sc[i])
+        t[i] = [float(f), float(f * ((a - 1) / X - 1 / s)), float(f * (mp.log(X / s) - mp.digamma(a))),
+                float(f * (X / s**2 - a / s))]
+    d["gamma_truth"], d["gamma_truth_grad"] = t[:, 0], t[:, 1:]
+    d["gamma_ref"] = ref("gamma_probability_density", 0, x, sh, sc)[0]
+    d["gamma_ref_grad"] = np.stack(ref("gamma_probability_density", 1, g, x, sh, sc), axis=1)
+    # chi-squared density
+    x2, df = lu(rng, 1e-3, 1e3, n), lu(rng, 0.2, 200.0, n)
+    x2[:6] = [0.0, 0.0, 0.0, -2.0, np.nan, 1.0]
+    df[:6] = [1.0, 2.0, 3.0, 4.0, 4.0, np.nan]
+    g2 = rng.standard_normal(n)
+    d["chi2_x"], d["chi2_df"], d["chi2_g"] = x2, df, g2
+    t2 = np.zeros((n, 3))
+    for i in range(n):
+        if np.isnan(x2[i]) or np.isnan(df[i]):
+            t2[i] = [np.nan, 0.0, 0.0]
+            continue
+        if x2[i] <= 0:
+            v = 0.0 if x2[i] < 0 else (np.inf if df[i] < 2 else (0.5 if df[i] == 2 else 0.0))
+            t2[i] = [v, 0.0, 0.0]
+            continue
+        k, X = mp.mpf(df[i]) / 2, mp.mpf(x2[i])
+        f = gpdf(X, k, 2)
+        t2[i] = [float(f), float(f * ((k - 1) / X - mp.mpf(1) / 2)), float(f * (mp.log(X / 2) - mp.digamma(k)) / 2)]
+    d["chi2_truth"], d["chi2_truth_grad"] = t2[:, 0], t2[:, 1:]
+    d["chi2_ref"] = ref("chi2_probability_density", 0, x2, df)[0]
+    d["chi2_ref_grad"] = np.stack(ref("chi2_probability_density", 1, g2, x2, df), axis=1)
+    # chi-squared survival: Q(df/2, x/2)
+    x3, df3 = lu(rng, 1e-3, 2e3, n), lu(rng, 0.2, 200.0, n)
+    x3[:3] = [0.0, -1.0, np.nan]
+    g3 = rng.standard_normal(n)
+    d["sf_x"], d["sf_df"], d["sf_g"] = x3, df3, g3
+    q = np.zeros(n)
+    for i in range(n):
+        if np.isnan(x3[i]):
+            q[i] = np.nan
+        elif x3[i] <= 0:
+            q[i] = 1.0
+        else:
+            q[i] = float(mp.gammainc(mp.mpf(df3[i]) / 2, mp.mpf(x3[i]) / 2, mp.inf, regularized=True))
+    d["sf_truth"] = q
+    with np.errstate(invalid="ignore"):
+        d["sf_truth_dx"] = np.array([0.0 if not v > 0 else -float(gpdf(v, mp.mpf(k) / 2, 2)) for v, k in zip(x3, df3)])
+    idx = np.arange(3, 203)
+    d["sf_ddf_idx"] = idx
+    d["sf_truth_ddf"] = np.array([-0.5 * _dP_da(df3[i] / 2, mp.mpf(x3[i]) / 2) for i in idx])
+    d["sf_ref"] = ref("chi2_survival", 0, x3, df3)[0]
+    d["sf_ref_grad"] = np.stack(ref("chi2_survival", 1, g3, x3, df3), axis=1)
+    np.savez_compressed(OUT / "probability_density.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density"]
     for w in which:
         globals()[w]()
         print("wrote", w)

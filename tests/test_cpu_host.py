@@ -37,6 +37,12 @@ REFERENCE_SCHEMAS = [
     "gamma_cumulative_distribution_backward(Tensor grad, Tensor x, Tensor shape, Tensor scale) -> (Tensor, Tensor, Tensor)",
     "poisson_cumulative_distribution(Tensor k, Tensor rate) -> Tensor",
     "poisson_cumulative_distribution_backward(Tensor grad, Tensor k, Tensor rate) -> (Tensor, Tensor)",
+    "chi2_survival(Tensor x, Tensor df) -> Tensor",
+    "chi2_survival_backward(Tensor grad, Tensor x, Tensor df) -> (Tensor, Tensor)",
+    "chi2_probability_density(Tensor x, Tensor df) -> Tensor",
+    "chi2_probability_density_backward(Tensor grad, Tensor x, Tensor df) -> (Tensor, Tensor)",
+    "gamma_probability_density(Tensor x, Tensor shape, Tensor scale) -> Tensor",
+    "gamma_probability_density_backward(Tensor grad, Tensor x, Tensor shape, Tensor scale) -> (Tensor, Tensor, Tensor)",
 ]
 
 

@@ -438,10 +438,12 @@ TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl("hypergeometric_2_f_1", t
 TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_autocast); }
 
 // ------------------------------------------- probability callers of P and Q
-// gamma / chi2 / poisson cumulative distributions (torchscience.cpp:1881-1924).
-// As in the reference (autograd/probability/*.h, cpu/probability/*.h), the
-// backward ops return gradients already reduced to the inputs' shapes and
-// have no double backward.
+// gamma / chi2 / poisson cumulative distributions, the chi2 survival function
+// and the gamma / chi2 densities (torchscience.cpp:1881-1924).  As in the
+// reference (autograd/probability/*.h, cpu/probability/*.h), the backward ops
+// return gradients already reduced to the inputs' shapes and have no double
+// backward.  Each op gets CUDA, Meta, CPU (an error) and Autograd kernels from
+// one macro per arity.
 namespace tsbh::prob {
 using T2 = std::tuple<at::Tensor, at::Tensor>;
 using T3 = std::tuple<at::Tensor, at::Tensor, at::Tensor>;
@@ -456,168 +458,111 @@ inline std::vector<at::Tensor> meta_grads(at::TensorList ins) {
 inline std::vector<at::Tensor> reduced_all(OpFn fn, const char* name, const at::Tensor& g, at::TensorList ins) {
   return run_reduced_backward(fn, name, g, ins, std::vector<bool>(ins.size(), true));
 }
-
-at::Tensor chi2_cuda(const at::Tensor& x, const at::Tensor& df) {
-  return run_pointwise(tsb_chi2_cumulative_distribution, "chi2_cumulative_distribution", {x, df}, 1)[0];
-}
-T2 chi2_backward_cuda(const at::Tensor& g, const at::Tensor& x, const at::Tensor& df) {
-  auto r = reduced_all(tsb_chi2_cumulative_distribution_backward, "chi2_cumulative_distribution_backward", g, {x, df});
-  return {r[0], r[1]};
-}
-at::Tensor gamma_cdf_cuda(const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
-  return run_pointwise(tsb_gamma_cumulative_distribution, "gamma_cumulative_distribution", {x, shape, scale}, 1)[0];
-}
-T3 gamma_cdf_backward_cuda(const at::Tensor& g, const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
-  auto r = reduced_all(tsb_gamma_cumulative_distribution_backward, "gamma_cumulative_distribution_backward", g,
-                       {x, shape, scale});
-  return {r[0], r[1], r[2]};
-}
-at::Tensor poisson_cuda(const at::Tensor& k, const at::Tensor& rate) {
-  return run_pointwise(tsb_poisson_cumulative_distribution, "poisson_cumulative_distribution", {k, rate}, 1)[0];
-}
-T2 poisson_backward_cuda(const at::Tensor& g, const at::Tensor& k, const at::Tensor& rate) {
-  auto r = reduced_all(tsb_poisson_cumulative_distribution_backward, "poisson_cumulative_distribution_backward", g,
-                       {k, rate});
-  return {r[0], r[1]};
-}
-
-at::Tensor chi2_meta(const at::Tensor& x, const at::Tensor& df) {
-  return meta_pointwise("chi2_cumulative_distribution", {x, df}, 1)[0];
-}
-T2 chi2_backward_meta(const at::Tensor& g, const at::Tensor& x, const at::Tensor& df) {
-  auto r = meta_grads({x, df});
-  return {r[0], r[1]};
-}
-at::Tensor gamma_cdf_meta(const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
-  return meta_pointwise("gamma_cumulative_distribution", {x, shape, scale}, 1)[0];
-}
-T3 gamma_cdf_backward_meta(const at::Tensor& g, const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
-  auto r = meta_grads({x, shape, scale});
-  return {r[0], r[1], r[2]};
-}
-at::Tensor poisson_meta(const at::Tensor& k, const at::Tensor& rate) {
-  return meta_pointwise("poisson_cumulative_distribution", {k, rate}, 1)[0];
-}
-T2 poisson_backward_meta(const at::Tensor& g, const at::Tensor& k, const at::Tensor& rate) {
-  auto r = meta_grads({k, rate});
-  return {r[0], r[1]};
-}
-
-at::Tensor chi2_cpu(const at::Tensor&, const at::Tensor&) { cpu_not_supported("chi2_cumulative_distribution"); }
-T2 chi2_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&) {
-  cpu_not_supported("chi2_cumulative_distribution_backward");
-}
-at::Tensor gamma_cdf_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&) {
-  cpu_not_supported("gamma_cumulative_distribution");
-}
-T3 gamma_cdf_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&) {
-  cpu_not_supported("gamma_cumulative_distribution_backward");
-}
-at::Tensor poisson_cpu(const at::Tensor&, const at::Tensor&) { cpu_not_supported("poisson_cumulative_distribution"); }
-T2 poisson_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&) {
-  cpu_not_supported("poisson_cumulative_distribution_backward");
-}
-
 template <typename Sig>
 inline auto op(const char* name) {
   return c10::Dispatcher::singleton().findSchemaOrThrow(name, "").typed<Sig>();
 }
+using A = const at::Tensor&;
 
-class Chi2Cdf : public torch::autograd::Function<Chi2Cdf> {
- public:
-  static at::Tensor forward(AutogradContext* ctx, const at::Tensor& x, const at::Tensor& df) {
-    ctx->save_for_backward({x, df});
-    at::AutoDispatchBelowAutograd guard;
-    static auto f = op<at::Tensor(const at::Tensor&, const at::Tensor&)>("torchscience::chi2_cumulative_distribution");
-    return f.call(x, df);
-  }
-  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
-    auto s = ctx->get_saved_variables();
-    if (!go[0].defined()) return {at::Tensor(), at::Tensor()};
-    at::AutoDispatchBelowAutograd guard;
-    static auto b = op<T2(const at::Tensor&, const at::Tensor&, const at::Tensor&)>(
-        "torchscience::chi2_cumulative_distribution_backward");
-    auto [gx, gdf] = b.call(go[0], s[0], s[1]);
-    return {gx, gdf};
-  }
-};
-class GammaCdf : public torch::autograd::Function<GammaCdf> {
- public:
-  static at::Tensor forward(AutogradContext* ctx, const at::Tensor& x, const at::Tensor& shape,
-                            const at::Tensor& scale) {
-    ctx->save_for_backward({x, shape, scale});
-    at::AutoDispatchBelowAutograd guard;
-    static auto f = op<at::Tensor(const at::Tensor&, const at::Tensor&, const at::Tensor&)>(
-        "torchscience::gamma_cumulative_distribution");
-    return f.call(x, shape, scale);
-  }
-  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
-    auto s = ctx->get_saved_variables();
-    if (!go[0].defined()) return {at::Tensor(), at::Tensor(), at::Tensor()};
-    at::AutoDispatchBelowAutograd guard;
-    static auto b = op<T3(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&)>(
-        "torchscience::gamma_cumulative_distribution_backward");
-    auto [gx, gs, gc] = b.call(go[0], s[0], s[1], s[2]);
-    return {gx, gs, gc};
-  }
-};
-class PoissonCdf : public torch::autograd::Function<PoissonCdf> {
- public:
-  static at::Tensor forward(AutogradContext* ctx, const at::Tensor& k, const at::Tensor& rate) {
-    ctx->save_for_backward({k, rate});
-    at::AutoDispatchBelowAutograd guard;
-    static auto f =
-        op<at::Tensor(const at::Tensor&, const at::Tensor&)>("torchscience::poisson_cumulative_distribution");
-    return f.call(k, rate);
-  }
-  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
-    auto s = ctx->get_saved_variables();
-    if (!go[0].defined()) return {at::Tensor(), at::Tensor()};
-    at::AutoDispatchBelowAutograd guard;
-    static auto b = op<T2(const at::Tensor&, const at::Tensor&, const at::Tensor&)>(
-        "torchscience::poisson_cumulative_distribution_backward");
-    auto [gk, gr] = b.call(go[0], s[0], s[1]);
-    return {gk, gr};
-  }
-};
+#define TSB_PROB_OP2(ID, NAME)                                                                               \
+  at::Tensor ID##_cuda(A a, A b) { return run_pointwise(tsb_##NAME, #NAME, {a, b}, 1)[0]; }                 \
+  T2 ID##_backward_cuda(A g, A a, A b) {                                                                     \
+    auto r = reduced_all(tsb_##NAME##_backward, #NAME "_backward", g, {a, b});                               \
+    return {r[0], r[1]};                                                                                     \
+  }                                                                                                          \
+  at::Tensor ID##_meta(A a, A b) { return meta_pointwise(#NAME, {a, b}, 1)[0]; }                            \
+  T2 ID##_backward_meta(A, A a, A b) {                                                                       \
+    auto r = meta_grads({a, b});                                                                             \
+    return {r[0], r[1]};                                                                                     \
+  }                                                                                                          \
+  at::Tensor ID##_cpu(A, A) { cpu_not_supported(#NAME); }                                                    \
+  T2 ID##_backward_cpu(A, A, A) { cpu_not_supported(#NAME "_backward"); }                                    \
+  class ID##_fn : public torch::autograd::Function<ID##_fn> {                                                \
+   public:                                                                                                   \
+    static at::Tensor forward(AutogradContext* ctx, A a, A b) {                                              \
+      ctx->save_for_backward({a, b});                                                                        \
+      at::AutoDispatchBelowAutograd guard;                                                                   \
+      static auto f = op<at::Tensor(A, A)>("torchscience::" #NAME);                                          \
+      return f.call(a, b);                                                                                   \
+    }                                                                                                        \
+    static variable_list backward(AutogradContext* ctx, const variable_list& go) {                           \
+      auto s = ctx->get_saved_variables();                                                                   \
+      if (!go[0].defined()) return {at::Tensor(), at::Tensor()};                                             \
+      at::AutoDispatchBelowAutograd guard;                                                                   \
+      static auto bw = op<T2(A, A, A)>("torchscience::" #NAME "_backward");                                  \
+      auto [ga, gb] = bw.call(go[0], s[0], s[1]);                                                            \
+      return {ga, gb};                                                                                       \
+    }                                                                                                        \
+  };                                                                                                         \
+  at::Tensor ID##_autograd(A a, A b) { return ID##_fn::apply(a, b); }
 
-at::Tensor chi2_autograd(const at::Tensor& x, const at::Tensor& df) { return Chi2Cdf::apply(x, df); }
-at::Tensor gamma_cdf_autograd(const at::Tensor& x, const at::Tensor& shape, const at::Tensor& scale) {
-  return GammaCdf::apply(x, shape, scale);
-}
-at::Tensor poisson_autograd(const at::Tensor& k, const at::Tensor& rate) { return PoissonCdf::apply(k, rate); }
+#define TSB_PROB_OP3(ID, NAME)                                                                               \
+  at::Tensor ID##_cuda(A a, A b, A c) { return run_pointwise(tsb_##NAME, #NAME, {a, b, c}, 1)[0]; }         \
+  T3 ID##_backward_cuda(A g, A a, A b, A c) {                                                                \
+    auto r = reduced_all(tsb_##NAME##_backward, #NAME "_backward", g, {a, b, c});                            \
+    return {r[0], r[1], r[2]};                                                                               \
+  }                                                                                                          \
+  at::Tensor ID##_meta(A a, A b, A c) { return meta_pointwise(#NAME, {a, b, c}, 1)[0]; }                    \
+  T3 ID##_backward_meta(A, A a, A b, A c) {                                                                  \
+    auto r = meta_grads({a, b, c});                                                                          \
+    return {r[0], r[1], r[2]};                                                                               \
+  }                                                                                                          \
+  at::Tensor ID##_cpu(A, A, A) { cpu_not_supported(#NAME); }                                                 \
+  T3 ID##_backward_cpu(A, A, A, A) { cpu_not_supported(#NAME "_backward"); }                                 \
+  class ID##_fn : public torch::autograd::Function<ID##_fn> {                                                \
+   public:                                                                                                   \
+    static at::Tensor forward(AutogradContext* ctx, A a, A b, A c) {                                         \
+      ctx->save_for_backward({a, b, c});                                                                     \
+      at::AutoDispatchBelowAutograd guard;                                                                   \
+      static auto f = op<at::Tensor(A, A, A)>("torchscience::" #NAME);                                       \
+      return f.call(a, b, c);                                                                                \
+    }                                                                                                        \
+    static variable_list backward(AutogradContext* ctx, const variable_list& go) {                           \
+      auto s = ctx->get_saved_variables();                                                                   \
+      if (!go[0].defined()) return {at::Tensor(), at::Tensor(), at::Tensor()};                               \
+      at::AutoDispatchBelowAutograd guard;                                                                   \
+      static auto bw = op<T3(A, A, A, A)>("torchscience::" #NAME "_backward");                               \
+      auto [ga, gb, gc] = bw.call(go[0], s[0], s[1], s[2]);                                                  \
+      return {ga, gb, gc};                                                                                   \
+    }                                                                                                        \
+  };                                                                                                         \
+  at::Tensor ID##_autograd(A a, A b, A c) { return ID##_fn::apply(a, b, c); }
+
+TSB_PROB_OP2(chi2_cdf, chi2_cumulative_distribution)
+TSB_PROB_OP3(gamma_cdf, gamma_cumulative_distribution)
+TSB_PROB_OP2(poisson_cdf, poisson_cumulative_distribution)
+TSB_PROB_OP2(chi2_sf, chi2_survival)
+TSB_PROB_OP3(gamma_pdf, gamma_probability_density)
+TSB_PROB_OP2(chi2_pdf, chi2_probability_density)
+#undef TSB_PROB_OP2
+#undef TSB_PROB_OP3
 }  // namespace tsbh::prob
 
+#define TSB_PROB_IMPL(ID, NAME, KEY)                   \
+  m.impl(#NAME, tsbh::prob::ID##_##KEY);              \
+  m.impl(#NAME "_backward", tsbh::prob::ID##_backward_##KEY);
+#define TSB_PROB_ALL(KEY)                                          \
+  TSB_PROB_IMPL(chi2_cdf, chi2_cumulative_distribution, KEY)       \
+  TSB_PROB_IMPL(gamma_cdf, gamma_cumulative_distribution, KEY)     \
+  TSB_PROB_IMPL(poisson_cdf, poisson_cumulative_distribution, KEY) \
+  TSB_PROB_IMPL(chi2_sf, chi2_survival, KEY)                       \
+  TSB_PROB_IMPL(gamma_pdf, gamma_probability_density, KEY)         \
+  TSB_PROB_IMPL(chi2_pdf, chi2_probability_density, KEY)
+
 TORCH_LIBRARY_FRAGMENT(torchscience, m) { TSB_DEFINE_PROBABILITY_SCHEMAS(m) }
-TORCH_LIBRARY_IMPL(torchscience, CUDA, m) {
-  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_cuda);
-  m.impl("chi2_cumulative_distribution_backward", tsbh::prob::chi2_backward_cuda);
-  m.impl("gamma_cumulative_distribution", tsbh::prob::gamma_cdf_cuda);
-  m.impl("gamma_cumulative_distribution_backward", tsbh::prob::gamma_cdf_backward_cuda);
-  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_cuda);
-  m.impl("poisson_cumulative_distribution_backward", tsbh::prob::poisson_backward_cuda);
-}
-TORCH_LIBRARY_IMPL(torchscience, Meta, m) {
-  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_meta);
-  m.impl("chi2_cumulative_distribution_backward", tsbh::prob::chi2_backward_meta);
-  m.impl("gamma_cumulative_distribution", tsbh::prob::gamma_cdf_meta);
-  m.impl("gamma_cumulative_distribution_backward", tsbh::prob::gamma_cdf_backward_meta);
-  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_meta);
-  m.impl("poisson_cumulative_distribution_backward", tsbh::prob::poisson_backward_meta);
-}
-TORCH_LIBRARY_IMPL(torchscience, CPU, m) {
-  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_cpu);
-  m.impl("chi2_cumulative_distribution_backward", tsbh::prob::chi2_backward_cpu);
-  m.impl("gamma_cumulative_distribution", tsbh::prob::gamma_cdf_cpu);
-  m.impl("gamma_cumulative_distribution_backward", tsbh::prob::gamma_cdf_backward_cpu);
-  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_cpu);
-  m.impl("poisson_cumulative_distribution_backward", tsbh::prob::poisson_backward_cpu);
-}
+TORCH_LIBRARY_IMPL(torchscience, CUDA, m) { TSB_PROB_ALL(cuda) }
+TORCH_LIBRARY_IMPL(torchscience, Meta, m) { TSB_PROB_ALL(meta) }
+TORCH_LIBRARY_IMPL(torchscience, CPU, m) { TSB_PROB_ALL(cpu) }
 TORCH_LIBRARY_IMPL(torchscience, Autograd, m) {
-  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_autograd);
+  m.impl("chi2_cumulative_distribution", tsbh::prob::chi2_cdf_autograd);
   m.impl("gamma_cumulative_distribution", tsbh::prob::gamma_cdf_autograd);
-  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_autograd);
+  m.impl("poisson_cumulative_distribution", tsbh::prob::poisson_cdf_autograd);
+  m.impl("chi2_survival", tsbh::prob::chi2_sf_autograd);
+  m.impl("gamma_probability_density", tsbh::prob::gamma_pdf_autograd);
+  m.impl("chi2_probability_density", tsbh::prob::chi2_pdf_autograd);
 }
+#undef TSB_PROB_ALL
+#undef TSB_PROB_IMPL
 
 // Library-level controls (not part of the reference's namespace).
 namespace tsbh {

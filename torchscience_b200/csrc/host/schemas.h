@@ -84,7 +84,7 @@
       "complete_legendre_elliptic_integral_e_backward_backward(Tensor gg_m, Tensor grad_output, Tensor m) -> "       \
       "(Tensor, Tensor)");
 
-// Schemas of the probability callers of the incomplete gamma (torchscience.cpp:1881-1882, 1909-1910,
+// Schemas of the probability callers of the incomplete gamma (torchscience.cpp:1881-1888, 1909-1912,
 // 1923-1924), registered by this package only.
 #define TSB_DEFINE_PROBABILITY_SCHEMAS(m)                                                                             \
   (m).def("chi2_cumulative_distribution(Tensor x, Tensor df) -> Tensor");                                            \
@@ -94,4 +94,12 @@
       "gamma_cumulative_distribution_backward(Tensor grad, Tensor x, Tensor shape, Tensor scale) -> (Tensor, Tensor, " \
       "Tensor)");                                                                                                    \
   (m).def("poisson_cumulative_distribution(Tensor k, Tensor rate) -> Tensor");                                       \
-  (m).def("poisson_cumulative_distribution_backward(Tensor grad, Tensor k, Tensor rate) -> (Tensor, Tensor)");
+  (m).def("poisson_cumulative_distribution_backward(Tensor grad, Tensor k, Tensor rate) -> (Tensor, Tensor)");       \
+  (m).def("chi2_survival(Tensor x, Tensor df) -> Tensor");                                                           \
+  (m).def("chi2_survival_backward(Tensor grad, Tensor x, Tensor df) -> (Tensor, Tensor)");                           \
+  (m).def("chi2_probability_density(Tensor x, Tensor df) -> Tensor");                                               \
+  (m).def("chi2_probability_density_backward(Tensor grad, Tensor x, Tensor df) -> (Tensor, Tensor)");               \
+  (m).def("gamma_probability_density(Tensor x, Tensor shape, Tensor scale) -> Tensor");                             \
+  (m).def(                                                                                                           \
+      "gamma_probability_density_backward(Tensor grad, Tensor x, Tensor shape, Tensor scale) -> (Tensor, Tensor, "   \
+      "Tensor)");
