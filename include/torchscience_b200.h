@@ -115,6 +115,22 @@ TSB_OP_SIGNATURE(tsb_digamma_backward_backward);
 TSB_OP_SIGNATURE(tsb_trigamma);
 TSB_OP_SIGNATURE(tsb_trigamma_backward);
 TSB_OP_SIGNATURE(tsb_trigamma_backward_backward);
+/* polygamma(n, z), order truncated toward zero, NaN for n <= -1: polygamma.h:45-62, schema
+ * torchscience.cpp:841-843; backward polygamma_backward.h:10-19 (outputs grad_n = 0,
+ * grad_z = grad·ψ^(n+1)(z)); double backward polygamma_backward_backward.h:10-22. */
+TSB_OP_SIGNATURE(tsb_polygamma);
+TSB_OP_SIGNATURE(tsb_polygamma_backward);
+TSB_OP_SIGNATURE(tsb_polygamma_backward_backward);
+/* log_beta(a, b) = ln|B(a, b)|: log_beta.h:10-13, schema torchscience.cpp:845-847; backward
+ * log_beta_backward.h:10-17; double backward log_beta_backward_backward.h:10-33. */
+TSB_OP_SIGNATURE(tsb_log_beta);
+TSB_OP_SIGNATURE(tsb_log_beta_backward);
+TSB_OP_SIGNATURE(tsb_log_beta_backward_backward);
+/* beta(a, b): beta.h:12-15, schema torchscience.cpp:825-827; backward beta_backward.h:13-27;
+ * double backward beta_backward_backward.h:10-30.  Signed for negative arguments. */
+TSB_OP_SIGNATURE(tsb_beta);
+TSB_OP_SIGNATURE(tsb_beta_backward);
+TSB_OP_SIGNATURE(tsb_beta_backward_backward);
 
 /* ---- Regularized incomplete gamma ------------------------------------- */
 /* regularized_gamma_p(a, x): regularized_gamma_p.h:57-71, schema

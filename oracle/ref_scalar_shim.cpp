@@ -27,6 +27,15 @@
 #include "kernel/probability/gamma_probability_density_backward.h"
 #include "kernel/probability/chi2_probability_density.h"
 #include "kernel/probability/chi2_probability_density_backward.h"
+#include "kernel/special_functions/beta.h"
+#include "kernel/special_functions/beta_backward.h"
+#include "kernel/special_functions/beta_backward_backward.h"
+#include "kernel/special_functions/log_beta.h"
+#include "kernel/special_functions/log_beta_backward.h"
+#include "kernel/special_functions/log_beta_backward_backward.h"
+#include "kernel/special_functions/polygamma.h"
+#include "kernel/special_functions/polygamma_backward.h"
+#include "kernel/special_functions/polygamma_backward_backward.h"
 #include "kernel/special_functions/bessel_j.h"
 #include "kernel/special_functions/bessel_j_0.h"
 #include "kernel/special_functions/bessel_j_0_backward.h"
@@ -155,6 +164,9 @@ static int eval_typed(const char* name, int pass, const void* const* in, void* c
   BINARY(bessel_y)
   BINARY(modified_bessel_i)
   BINARY(modified_bessel_k)
+  BINARY(log_beta)
+  BINARY(beta)
+  BINARY(polygamma)
   if (std::strcmp(name, "gamma_cumulative_distribution") == 0) {
     if (pass == 0) LOOP(pr::gamma_cumulative_distribution(ARG(0), ARG(1), ARG(2)));
     if (pass == 1) LOOP(pr::gamma_cumulative_distribution_backward(ARG(0), ARG(1), ARG(2), ARG(3)));

@@ -402,8 +402,62 @@ def probability_density():
     np.savez_compressed(OUT / "probability_density.npz", **d)
 
 
+def beta_family():
+    """log_beta, beta and polygamma: seeded positive arguments over [1e-3, 1e6]
+    (with a block of b << a, where ψ(a) - ψ(a+b) cancels), negative
+    non-integer a, the reference's special points, and orders 0..30 of ψ^(n)
+    at positive and negative z; mpmath values (40 digits) of ln|B|, B, the
+    ψ and ψ' differences, ψ^(n), ψ^(n+1), ψ^(n+2); the reference's outputs."""
+    rng = np.random.default_rng(10)
+    n = 2000
+    a = np.concatenate([lu(rng, 1e-3, 1e6, n), rng.uniform(0.05, 20.0, 400), -rng.uniform(0.0, 10.0, 200) - 1e-3])
+    b = np.concatenate([lu(rng, 1e-3, 1e6, n), rng.uniform(0.05, 20.0, 400), rng.uniform(0.1, 10.0, 200)])
+    b[:300] = a[:300] * lu(rng, 1e-12, 1e-3, 300)
+    sa = np.array([0.0, -1.0, 1.0, 0.5, 2.0, np.nan, 1.0, np.inf, 3.0])
+    sb = np.array([1.0, 1.0, 1.0, 0.5, 3.0, 1.0, np.nan, 2.0, 1e-300])
+    d = {"a": a, "b": b, "special_a": sa, "special_b": sb, "g": rng.standard_normal(a.size)}
+    cols = {k: [] for k in ("lnb", "b", "da", "db", "daa", "dbb", "dab")}
+    for x, y in zip(a, b):
+        X, Y = mp.mpf(x), mp.mpf(y)
+        B = mp.gamma(X) * mp.gamma(Y) / mp.gamma(X + Y) if x < 0 else mp.beta(X, Y)
+        cols["lnb"].append(float(mp.log(abs(B))))
+        cols["b"].append(float(B))
+        cols["da"].append(float(mp.digamma(X) - mp.digamma(X + Y)))
+        cols["db"].append(float(mp.digamma(Y) - mp.digamma(X + Y)))
+        cols["daa"].append(float(mp.psi(1, X) - mp.psi(1, X + Y)))
+        cols["dbb"].append(float(mp.psi(1, Y) - mp.psi(1, X + Y)))
+        cols["dab"].append(float(-mp.psi(1, X + Y)))
+    for k, v in cols.items():
+        d[f"truth_{k}"] = np.array(v)
+    gg = rng.standard_normal((2, a.size))
+    d["gg"] = gg
+    for nm in ("log_beta", "beta"):
+        d[f"ref_{nm}"] = ref(nm, 0, a, b)[0]
+        d[f"ref_{nm}_grad"] = np.stack(ref(nm, 1, d["g"], a, b), axis=1)
+        d[f"ref_{nm}_bb"] = np.stack(ref(nm, 2, gg[0], gg[1], d["g"], a, b), axis=1)
+        d[f"ref_{nm}_special"] = ref(nm, 0, sa, sb)[0]
+    # polygamma
+    m = 1500
+    pn = np.concatenate([rng.integers(0, 31, m).astype(float), [2.7, -0.5, -1.0, 4.0, 5.0, 4.0, 1.0, 2.0, 6.0]])
+    pz = np.concatenate([lu(rng, 1e-3, 1e3, m - 300), -rng.uniform(0.0, 30.0, 300) - 1e-3,
+                         [2.0, 2.0, 2.0, 0.0, -3.0, 2.0, 1.0, 0.5, -0.5]])
+    d["pg_n"], d["pg_z"] = pn, pz
+    t0, t1, t2 = [], [], []
+    for k, z in zip(pn, pz):
+        order = int(k) if k > -1 else -1
+        Z = mp.mpf(z)
+        pole = z <= 0 and z == int(z)
+        for lst, o in ((t0, order), (t1, int(k + 1) if k + 1 > -1 else -1), (t2, int(k + 2) if k + 2 > -1 else -1)):
+            lst.append(np.nan if o < 0 or pole else float(mp.polygamma(o, Z)))
+    d["pg_truth"], d["pg_truth_d1"], d["pg_truth_d2"] = np.array(t0), np.array(t1), np.array(t2)
+    d["pg_g"] = rng.standard_normal(pn.size)
+    d["pg_ref"] = ref("polygamma", 0, pn, pz)[0]
+    d["pg_ref_grad"] = np.stack(ref("polygamma", 1, d["pg_g"], pn, pz), axis=1)
+    np.savez_compressed(OUT / "beta_family.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family"]
     for w in which:
         globals()[w]()
         print("wrote", w)

@@ -21,6 +21,12 @@ REFERENCE_SCHEMAS = [
     "regularized_gamma_p_backward_backward(Tensor grad_grad_a, Tensor grad_grad_x, Tensor grad, Tensor a, Tensor x) -> (Tensor, Tensor, Tensor)",
     "regularized_gamma_q(Tensor a, Tensor x) -> Tensor",
     "bessel_j_0(Tensor z) -> Tensor",
+    "beta(Tensor a, Tensor b) -> Tensor",
+    "beta_backward_backward(Tensor gg_a, Tensor gg_b, Tensor grad_output, Tensor a, Tensor b) -> (Tensor, Tensor, Tensor)",
+    "polygamma(Tensor n, Tensor z) -> Tensor",
+    "polygamma_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor, Tensor)",
+    "log_beta(Tensor a, Tensor b) -> Tensor",
+    "log_beta_backward(Tensor grad_output, Tensor a, Tensor b) -> (Tensor, Tensor)",
     "bessel_j(Tensor n, Tensor z) -> Tensor",
     "bessel_j_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)",
     "bessel_y(Tensor n, Tensor z) -> Tensor",

@@ -272,6 +272,9 @@ TSBH_BINARY_OP(regularized_gamma_p, RegularizedGammaP, a, x, tsb_regularized_gam
                tsb_regularized_gamma_p_backward_backward)
 TSBH_BINARY_OP(regularized_gamma_q, RegularizedGammaQ, a, x, tsb_regularized_gamma_q, tsb_regularized_gamma_q_backward,
                tsb_regularized_gamma_q_backward_backward)
+TSBH_BINARY_OP(polygamma, Polygamma, n, z, tsb_polygamma, tsb_polygamma_backward, tsb_polygamma_backward_backward)
+TSBH_BINARY_OP(log_beta, LogBeta, a, b, tsb_log_beta, tsb_log_beta_backward, tsb_log_beta_backward_backward)
+TSBH_BINARY_OP(beta, Beta, a, b, tsb_beta, tsb_beta_backward, tsb_beta_backward_backward)
 TSBH_UNARY_OP(bessel_j_0, BesselJ0, z, tsb_bessel_j_0, tsb_bessel_j_0_backward, tsb_bessel_j_0_backward_backward)
 TSBH_BINARY_OP(bessel_j, BesselJ, n, z, tsb_bessel_j, tsb_bessel_j_backward, tsb_bessel_j_backward_backward)
 TSBH_BINARY_OP(bessel_y, BesselY, n, z, tsb_bessel_y, tsb_bessel_y_backward, tsb_bessel_y_backward_backward)

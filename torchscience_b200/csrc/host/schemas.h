@@ -19,6 +19,24 @@
   (m).def("trigamma(Tensor z) -> Tensor");                                                                           \
   (m).def("trigamma_backward(Tensor grad_output, Tensor z) -> Tensor");                                              \
   (m).def("trigamma_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");              \
+  /* torchscience.cpp:825-827 */                                                                                     \
+  (m).def("beta(Tensor a, Tensor b) -> Tensor");                                                                     \
+  (m).def("beta_backward(Tensor grad_output, Tensor a, Tensor b) -> (Tensor, Tensor)");                              \
+  (m).def(                                                                                                           \
+      "beta_backward_backward(Tensor gg_a, Tensor gg_b, Tensor grad_output, Tensor a, Tensor b) -> (Tensor, Tensor, " \
+      "Tensor)");                                                                                                    \
+  /* torchscience.cpp:841-843 */                                                                                     \
+  (m).def("polygamma(Tensor n, Tensor z) -> Tensor");                                                                \
+  (m).def("polygamma_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                         \
+  (m).def(                                                                                                           \
+      "polygamma_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> (Tensor, "    \
+      "Tensor, Tensor)");                                                                                            \
+  /* torchscience.cpp:845-847 */                                                                                     \
+  (m).def("log_beta(Tensor a, Tensor b) -> Tensor");                                                                 \
+  (m).def("log_beta_backward(Tensor grad_output, Tensor a, Tensor b) -> (Tensor, Tensor)");                          \
+  (m).def(                                                                                                           \
+      "log_beta_backward_backward(Tensor gg_a, Tensor gg_b, Tensor grad_output, Tensor a, Tensor b) -> (Tensor, "     \
+      "Tensor, Tensor)");                                                                                            \
   /* torchscience.cpp:837-839 */                                                                                     \
   (m).def("hypergeometric_2_f_1(Tensor a, Tensor b, Tensor c, Tensor z) -> Tensor");                                 \
   (m).def(                                                                                                           \

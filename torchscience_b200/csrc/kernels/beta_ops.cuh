@@ -1,0 +1,127 @@
+// log_beta, beta and polygamma: functors of the forward, backward and
+// double-backward entry points (reference: log_beta.h:10-13,
+// log_beta_backward.h:10-17, log_beta_backward_backward.h:10-33,
+// beta.h:12-15, beta_backward.h:13-27, beta_backward_backward.h:10-30,
+// polygamma.h:45-62, polygamma_backward.h:10-19,
+// polygamma_backward_backward.h:10-22).  Every argument costs about the same
+// (no region split); float data is evaluated in FP64 and rounded once.
+#pragma once
+
+#include "beta_math.cuh"
+#include "dispatch.cuh"
+
+namespace tsb {
+
+// Second-order pieces of ln B: ∂a, ∂b, ∂aa, ∂bb, ∂ab.
+struct LogBetaDerivs {
+  double da, db, daa, dbb, dab;
+};
+__device__ inline LogBetaDerivs log_beta_derivs(double a, double b) {
+  return {log_beta_da(a, b), log_beta_da(b, a), log_beta_daa(a, b), log_beta_daa(b, a), -trigamma_d(a + b)};
+}
+
+template <typename T_>
+struct LogBetaFwd {
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) { out[0] = (T)log_beta_d(in[0], in[1]); }
+};
+
+template <typename T_>
+struct LogBetaBwd {  // in = {grad, a, b}, out = {grad_a, grad_b}
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t mask) {
+    const double g = in[0], a = in[1], b = in[2];
+    out[0] = (mask & 1u) ? (T)(g * log_beta_da(a, b)) : T(0);
+    out[1] = (mask & 2u) ? (T)(g * log_beta_da(b, a)) : T(0);
+  }
+};
+
+template <typename T_>
+struct LogBetaBwdBwd {  // in = {gg_a, gg_b, grad, a, b}, out = {grad_grad_output, grad_a, grad_b}
+  using T = T_;
+  static constexpr int NIN = 5, NOUT = 3, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double gga = in[0], ggb = in[1], g = in[2];
+    const LogBetaDerivs d = log_beta_derivs(in[3], in[4]);
+    out[0] = (T)(gga * d.da + ggb * d.db);
+    out[1] = (T)(g * (gga * d.daa + ggb * d.dab));
+    out[2] = (T)(g * (gga * d.dab + ggb * d.dbb));
+  }
+};
+
+template <typename T_>
+struct BetaFwd {
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) { out[0] = (T)beta_d(in[0], in[1]); }
+};
+
+template <typename T_>
+struct BetaBwd {  // in = {grad, a, b}: ∂B/∂a = B (ψ(a) - ψ(a+b))
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t mask) {
+    const double g = in[0], a = in[1], b = in[2], gB = g * beta_d(a, b);
+    out[0] = (mask & 1u) ? (T)(gB * log_beta_da(a, b)) : T(0);
+    out[1] = (mask & 2u) ? (T)(gB * log_beta_da(b, a)) : T(0);
+  }
+};
+
+template <typename T_>
+struct BetaBwdBwd {  // ∂²B = B (∂ ln B ∂ ln B + ∂² ln B)
+  using T = T_;
+  static constexpr int NIN = 5, NOUT = 3, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double gga = in[0], ggb = in[1], g = in[2], a = in[3], b = in[4];
+    const double B = beta_d(a, b);
+    const LogBetaDerivs d = log_beta_derivs(a, b);
+    const double haa = B * fma(d.da, d.da, d.daa), hab = B * fma(d.da, d.db, d.dab), hbb = B * fma(d.db, d.db, d.dbb);
+    out[0] = (T)(B * (gga * d.da + ggb * d.db));
+    out[1] = (T)(g * (gga * haa + ggb * hab));
+    out[2] = (T)(g * (gga * hab + ggb * hbb));
+  }
+};
+
+template <typename T_>
+struct PolygammaFwd {  // in = {n, z}
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    out[0] = (T)polygamma_d(polygamma_order(in[0]), in[1]);
+  }
+};
+
+template <typename T_>
+struct PolygammaBwd {  // in = {grad, n, z}, out = {grad_n = 0, grad_z = grad·ψ^(n+1)(z)}
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t mask) {
+    out[0] = T(0);
+    out[1] = (mask & 2u) ? (T)((double)in[0] * polygamma_d(polygamma_order((double)in[1] + 1.0), in[2])) : T(0);
+  }
+};
+
+template <typename T_>
+struct PolygammaBwdBwd {  // in = {gg_n, gg_z, grad, n, z}
+  using T = T_;
+  static constexpr int NIN = 5, NOUT = 3, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double ggz = in[1], g = in[2], n = in[3], z = in[4];
+    out[0] = (T)(ggz * polygamma_d(polygamma_order(n + 1.0), z));
+    out[1] = T(0);
+    out[2] = (T)(ggz * g * polygamma_d(polygamma_order(n + 2.0), z));
+  }
+};
+
+}  // namespace tsb

@@ -127,18 +127,47 @@ def hypergeometric_2_f_1(a: Tensor, b: Tensor, c: Tensor, z: Tensor) -> Tensor:
     return torch.ops.torchscience.hypergeometric_2_f_1(a, b, c, z)
 
 
+def polygamma(n: Tensor, z: Tensor) -> Tensor:
+    """Polygamma ψ^(n)(z), the order read as the reference reads it (truncated
+    toward zero; NaN for n <= -1).  n >= 4 uses the Hurwitz zeta
+    (-1)^(n+1) n! ζ(n+1, z) by Euler–Maclaurin summation.  Same signature and
+    semantics as the reference wrapper (src/torchscience/special_functions/_polygamma.py:5).
+    """
+    return torch.ops.torchscience.polygamma(n, z)
+
+
+def log_beta(a: Tensor, b: Tensor) -> Tensor:
+    """ln|B(a, b)| = lnΓ(a) + lnΓ(b) - lnΓ(a+b), formed without the
+    cancellation of those sums for large arguments; +inf where Γ(a) or Γ(b)
+    has a pole.  Same signature as the reference wrapper
+    (src/torchscience/special_functions/_log_beta.py:5).
+    """
+    return torch.ops.torchscience.log_beta(a, b)
+
+
+def beta(a: Tensor, b: Tensor) -> Tensor:
+    """Beta function B(a, b) = Γ(a)Γ(b)/Γ(a+b), with its sign for negative
+    arguments (the reference returns exp(ln|B|)).  Same signature as the
+    reference wrapper (src/torchscience/special_functions/_beta.py:5).
+    """
+    return torch.ops.torchscience.beta(a, b)
+
+
 __all__ = [
     "bessel_j",
     "bessel_j_0",
     "bessel_y",
+    "beta",
     "complete_legendre_elliptic_integral_e",
     "complete_legendre_elliptic_integral_k",
     "digamma",
     "gamma",
     "hypergeometric_2_f_1",
+    "log_beta",
     "log_gamma",
     "modified_bessel_i",
     "modified_bessel_k",
+    "polygamma",
     "regularized_gamma_p",
     "regularized_gamma_q",
     "trigamma",
