@@ -169,6 +169,35 @@ int32_t tsb_regularized_gamma_p_backward_noalloc(const tsb_tensor* in, int32_t n
 TSB_OP_SIGNATURE(tsb_bessel_j_0);
 TSB_OP_SIGNATURE(tsb_bessel_j_0_backward);
 TSB_OP_SIGNATURE(tsb_bessel_j_0_backward_backward);
+/* Integer orders 0 and 1 as unary ops; double backward gives {gg·f'(z), gg·grad·f''(z)}. */
+/* bessel_j_1(z): bessel_j_1.h:93-117, schema torchscience.cpp:877-879; J1 (odd); backward J0 - J1/z (1/2 at 0). */
+TSB_OP_SIGNATURE(tsb_bessel_j_1);
+TSB_OP_SIGNATURE(tsb_bessel_j_1_backward);
+TSB_OP_SIGNATURE(tsb_bessel_j_1_backward_backward);
+/* bessel_y_0(z): bessel_y_0.h:95-116, schema torchscience.cpp:882-884; Y0: NaN for z < 0, -inf at 0; backward -Y1 (NaN for z <= 0). */
+TSB_OP_SIGNATURE(tsb_bessel_y_0);
+TSB_OP_SIGNATURE(tsb_bessel_y_0_backward);
+TSB_OP_SIGNATURE(tsb_bessel_y_0_backward_backward);
+/* bessel_y_1(z): bessel_y_1.h:94-116, schema torchscience.cpp:887-889; Y1: NaN for z < 0, -inf at 0; backward Y0 - Y1/z (NaN for z <= 0). */
+TSB_OP_SIGNATURE(tsb_bessel_y_1);
+TSB_OP_SIGNATURE(tsb_bessel_y_1_backward);
+TSB_OP_SIGNATURE(tsb_bessel_y_1_backward_backward);
+/* modified_bessel_i_0(z): modified_bessel_i_0.h:71-86, schema torchscience.cpp:862-864; I0 (even); backward I1. */
+TSB_OP_SIGNATURE(tsb_modified_bessel_i_0);
+TSB_OP_SIGNATURE(tsb_modified_bessel_i_0_backward);
+TSB_OP_SIGNATURE(tsb_modified_bessel_i_0_backward_backward);
+/* modified_bessel_i_1(z): modified_bessel_i_1.h:55-74, schema torchscience.cpp:867-869; I1 (odd); backward I0 - I1/z (1/2 at 0). */
+TSB_OP_SIGNATURE(tsb_modified_bessel_i_1);
+TSB_OP_SIGNATURE(tsb_modified_bessel_i_1_backward);
+TSB_OP_SIGNATURE(tsb_modified_bessel_i_1_backward_backward);
+/* modified_bessel_k_0(z): modified_bessel_k_0.h:50-76, schema torchscience.cpp:892-894; K0: NaN for z < 0, +inf at 0; backward -K1 (NaN for z <= 0). */
+TSB_OP_SIGNATURE(tsb_modified_bessel_k_0);
+TSB_OP_SIGNATURE(tsb_modified_bessel_k_0_backward);
+TSB_OP_SIGNATURE(tsb_modified_bessel_k_0_backward_backward);
+/* modified_bessel_k_1(z): modified_bessel_k_1.h:51-78, schema torchscience.cpp:897-899; K1: NaN for z < 0, +inf at 0; backward -K0 - K1/z (NaN for z <= 0). */
+TSB_OP_SIGNATURE(tsb_modified_bessel_k_1);
+TSB_OP_SIGNATURE(tsb_modified_bessel_k_1_backward);
+TSB_OP_SIGNATURE(tsb_modified_bessel_k_1_backward_backward);
 /* bessel_j(n, z): bessel_j.h:240-316, schema torchscience.cpp:902-904;
  * backward bessel_j_backward.h:51-63 (grad_n, grad_z), backward_backward bessel_j_backward_backward.h. */
 TSB_OP_SIGNATURE(tsb_bessel_j);

@@ -456,8 +456,55 @@ def beta_family():
     np.savez_compressed(OUT / "beta_family.npz", **d)
 
 
+BESSEL_INT = {  # name: (mpmath function, order, domain sign: 1 = z > 0 only, 0 = both signs)
+    "bessel_j_1": (mp.besselj, 1, 0), "bessel_y_0": (mp.bessely, 0, 1), "bessel_y_1": (mp.bessely, 1, 1),
+    "modified_bessel_i_0": (mp.besseli, 0, 0), "modified_bessel_i_1": (mp.besseli, 1, 0),
+    "modified_bessel_k_0": (mp.besselk, 0, 1), "modified_bessel_k_1": (mp.besselk, 1, 1)}
+
+
+def bessel_int():
+    """Integer orders 0 and 1 as unary ops: z log-uniform over [1e-6, 1e3] (to
+    700 for I), z in [0, 60], negative z for the odd/even functions, points
+    within relative 1e-10..1e-4 of the first zeros of J1, Y0, Y1; mpmath values
+    (40 digits) of f, f', f''; the reference's forward, backward and double
+    backward outputs; the reference's special points."""
+    rng = np.random.default_rng(11)
+    d = {}
+    for name, (fn, order, pos_only) in BESSEL_INT.items():
+        hi = 700.0 if name.startswith("modified_bessel_i") else 1e3
+        z = np.concatenate([lu(rng, 1e-6, hi, 800), rng.uniform(0.0, 60.0, 400)])
+        if not pos_only:
+            z = np.concatenate([z, -lu(rng, 1e-6, 60.0, 200)])
+        if name in ("bessel_j_1", "bessel_y_0", "bessel_y_1"):
+            kind = {"bessel_j_1": (mp.besseljzero, 1), "bessel_y_0": (mp.besselyzero, 0), "bessel_y_1": (mp.besselyzero, 1)}[name]
+            zs = np.array([float(kind[0](kind[1], k)) for k in range(1, 16)])
+            z = np.concatenate([z, np.repeat(zs, 6) * (1 + rng.choice([-1.0, 1.0], 90) * lu(rng, 1e-10, 1e-4, 90))])
+        g, gg = rng.standard_normal(z.size), rng.standard_normal(z.size)
+        if name.startswith("modified_bessel_k"):  # mpmath's besselk takes no derivative order: closed forms
+            def kd(v, n=order):
+                v = mp.mpf(v)
+                k0, k1 = mp.besselk(0, v), mp.besselk(1, v)
+                if n == 0:
+                    return [k0, -k1, k0 + k1 / v]
+                return [k1, -k0 - k1 / v, k1 + k0 / v + 2 * k1 / v**2]
+
+            t = np.array([[float(x) for x in kd(v)] for v in z])
+        else:  # mpmath's derivative formulas return an mpc (zero imaginary part) for some z < 0
+            t = np.array([[float(mp.re(fn(order, mp.mpf(v), derivative=k))) for k in range(3)] for v in z])
+        d[f"{name}_z"], d[f"{name}_g"], d[f"{name}_gg"] = z, g, gg
+        d[f"{name}_truth"] = t
+        d[f"{name}_ref"] = ref(name, 0, z)[0]
+        d[f"{name}_ref_grad"] = ref(name, 1, g, z)[0]
+        d[f"{name}_ref_bb"] = np.stack(ref(name, 2, gg, g, z), axis=1)
+        sz = np.array([0.0, -0.0, -1.0, np.inf, -np.inf, np.nan, 1e-13])
+        d[f"{name}_special_z"] = sz
+        d[f"{name}_special_ref"] = ref(name, 0, sz)[0]
+        d[f"{name}_special_ref_grad"] = ref(name, 1, np.ones_like(sz), sz)[0]
+    np.savez_compressed(OUT / "bessel_int.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family", "bessel_int"]
     for w in which:
         globals()[w]()
         print("wrote", w)

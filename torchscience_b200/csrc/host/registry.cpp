@@ -276,6 +276,13 @@ TSBH_BINARY_OP(polygamma, Polygamma, n, z, tsb_polygamma, tsb_polygamma_backward
 TSBH_BINARY_OP(log_beta, LogBeta, a, b, tsb_log_beta, tsb_log_beta_backward, tsb_log_beta_backward_backward)
 TSBH_BINARY_OP(beta, Beta, a, b, tsb_beta, tsb_beta_backward, tsb_beta_backward_backward)
 TSBH_UNARY_OP(bessel_j_0, BesselJ0, z, tsb_bessel_j_0, tsb_bessel_j_0_backward, tsb_bessel_j_0_backward_backward)
+TSBH_UNARY_OP(bessel_j_1, BesselJ1, z, tsb_bessel_j_1, tsb_bessel_j_1_backward, tsb_bessel_j_1_backward_backward)
+TSBH_UNARY_OP(bessel_y_0, BesselY0, z, tsb_bessel_y_0, tsb_bessel_y_0_backward, tsb_bessel_y_0_backward_backward)
+TSBH_UNARY_OP(bessel_y_1, BesselY1, z, tsb_bessel_y_1, tsb_bessel_y_1_backward, tsb_bessel_y_1_backward_backward)
+TSBH_UNARY_OP(modified_bessel_i_0, ModifiedBesselI0, z, tsb_modified_bessel_i_0, tsb_modified_bessel_i_0_backward, tsb_modified_bessel_i_0_backward_backward)
+TSBH_UNARY_OP(modified_bessel_i_1, ModifiedBesselI1, z, tsb_modified_bessel_i_1, tsb_modified_bessel_i_1_backward, tsb_modified_bessel_i_1_backward_backward)
+TSBH_UNARY_OP(modified_bessel_k_0, ModifiedBesselK0, z, tsb_modified_bessel_k_0, tsb_modified_bessel_k_0_backward, tsb_modified_bessel_k_0_backward_backward)
+TSBH_UNARY_OP(modified_bessel_k_1, ModifiedBesselK1, z, tsb_modified_bessel_k_1, tsb_modified_bessel_k_1_backward, tsb_modified_bessel_k_1_backward_backward)
 TSBH_BINARY_OP(bessel_j, BesselJ, n, z, tsb_bessel_j, tsb_bessel_j_backward, tsb_bessel_j_backward_backward)
 TSBH_BINARY_OP(bessel_y, BesselY, n, z, tsb_bessel_y, tsb_bessel_y_backward, tsb_bessel_y_backward_backward)
 TSBH_BINARY_OP(modified_bessel_i, ModifiedBesselI, n, z, tsb_modified_bessel_i, tsb_modified_bessel_i_backward,

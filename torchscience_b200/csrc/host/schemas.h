@@ -37,6 +37,34 @@
   (m).def(                                                                                                           \
       "log_beta_backward_backward(Tensor gg_a, Tensor gg_b, Tensor grad_output, Tensor a, Tensor b) -> (Tensor, "     \
       "Tensor, Tensor)");                                                                                            \
+  /* torchscience.cpp:877-879 */                                                                                       \
+  (m).def("bessel_j_1(Tensor z) -> Tensor");                                                                           \
+  (m).def("bessel_j_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                              \
+  (m).def("bessel_j_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");              \
+  /* torchscience.cpp:882-884 */                                                                                       \
+  (m).def("bessel_y_0(Tensor z) -> Tensor");                                                                           \
+  (m).def("bessel_y_0_backward(Tensor grad_output, Tensor z) -> Tensor");                                              \
+  (m).def("bessel_y_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");              \
+  /* torchscience.cpp:887-889 */                                                                                       \
+  (m).def("bessel_y_1(Tensor z) -> Tensor");                                                                           \
+  (m).def("bessel_y_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                              \
+  (m).def("bessel_y_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");              \
+  /* torchscience.cpp:862-864 */                                                                                       \
+  (m).def("modified_bessel_i_0(Tensor z) -> Tensor");                                                                  \
+  (m).def("modified_bessel_i_0_backward(Tensor grad_output, Tensor z) -> Tensor");                                     \
+  (m).def("modified_bessel_i_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");     \
+  /* torchscience.cpp:867-869 */                                                                                       \
+  (m).def("modified_bessel_i_1(Tensor z) -> Tensor");                                                                  \
+  (m).def("modified_bessel_i_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                     \
+  (m).def("modified_bessel_i_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");     \
+  /* torchscience.cpp:892-894 */                                                                                       \
+  (m).def("modified_bessel_k_0(Tensor z) -> Tensor");                                                                  \
+  (m).def("modified_bessel_k_0_backward(Tensor grad_output, Tensor z) -> Tensor");                                     \
+  (m).def("modified_bessel_k_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");     \
+  /* torchscience.cpp:897-899 */                                                                                       \
+  (m).def("modified_bessel_k_1(Tensor z) -> Tensor");                                                                  \
+  (m).def("modified_bessel_k_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                     \
+  (m).def("modified_bessel_k_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");     \
   /* torchscience.cpp:837-839 */                                                                                     \
   (m).def("hypergeometric_2_f_1(Tensor a, Tensor b, Tensor c, Tensor z) -> Tensor");                                 \
   (m).def(                                                                                                           \

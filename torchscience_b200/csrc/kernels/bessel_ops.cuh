@@ -311,3 +311,90 @@ TSB_BESSEL_ALIASES(BesselI, kBI)
 TSB_BESSEL_ALIASES(BesselK, kBK)
 
 }  // namespace tsb
+
+namespace tsb {
+
+// ---- integer orders 0 and 1 as unary ops: bessel_j_1, bessel_y_0, bessel_y_1,
+// modified_bessel_i_0, modified_bessel_i_1, modified_bessel_k_0, modified_bessel_k_1.
+// Values, first and second derivatives with the reference's conventions
+// (bessel_j_1.h:93-117, bessel_y_0.h:95-116, bessel_y_1.h:94-116,
+// modified_bessel_i_0.h:71-86, modified_bessel_i_1.h:55-74,
+// modified_bessel_k_0.h:50-76, modified_bessel_k_1.h:51-78 and their
+// _backward / _backward_backward files): Y and K are NaN for z < 0 and
+// ∓inf / +inf at 0 with NaN derivatives there; J1, I1 are odd and I0 even;
+// J1'(0) = I1'(0) = 1/2, J1''(0) = I1''(0) = 0, I0''(0) = 1/2.  J1 comes
+// from the order-0/1 path, the others from the real-order evaluator at
+// ν = 0, 1; second derivatives from Bessel's equation.
+struct BesselIntVals {
+  double v, d, d2;
+};
+
+template <int KIND, int ORDER>
+__device__ inline BesselIntVals bessel_int_vals(double z, bool need_d2) {
+  const double nan = CUDART_NAN, inf = CUDART_INF;
+  if (isnan(z)) return {z, z, z};
+  if (KIND == kBY || KIND == kBK) {
+    if (z < 0.0) return {nan, nan, nan};
+    if (z == 0.0) return {KIND == kBY ? -inf : inf, nan, nan};
+  }
+  if (z == 0.0) {  // J1, I0, I1
+    if (KIND == kBI && ORDER == 0) return {1.0, 0.0, 0.5};
+    return {0.0, 0.5, 0.0};
+  }
+  BV<double> b;
+  if (KIND == kBJ) {
+    if (isinf(z)) return {0.0, 0.0, 0.0};
+    const J01 r = bessel_j01<true, true, TSB_B01_UNROLL>(z);
+    b = {r.j1, r.j0 - r.j1 / z};
+  } else {
+    b = bessel_eval<double, KIND>((double)ORDER, z);
+  }
+  const double d2 = need_d2 ? (isinf(z) ? (KIND == kBI ? inf : 0.0) : bessel_d2<double, KIND>((double)ORDER, z, b)) : 0.0;
+  return {b.v, b.d, d2};
+}
+
+template <int KIND, int ORDER, typename T_>
+struct BesselIntFwd {
+  using T = T_;
+  static constexpr int NIN = 1, NOUT = 1, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    out[0] = (T)bessel_int_vals<KIND, ORDER>((double)in[0], false).v;
+  }
+};
+template <int KIND, int ORDER, typename T_>
+struct BesselIntBwd {  // in = {grad, z}
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    out[0] = (T)((double)in[0] * bessel_int_vals<KIND, ORDER>((double)in[1], false).d);
+  }
+};
+template <int KIND, int ORDER, typename T_>
+struct BesselIntBwdBwd {  // in = {gg, grad, z}: {gg·f'(z), gg·grad·f''(z)}
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double gg = in[0], g = in[1];
+    const BesselIntVals f = bessel_int_vals<KIND, ORDER>((double)in[2], true);
+    out[0] = (T)(gg * f.d);
+    out[1] = (T)(gg * g * f.d2);
+  }
+};
+
+#define TSB_BESSEL_INT_ALIASES(Name, KIND, ORDER)                                          \
+  template <typename T> using Name##Fwd = BesselIntFwd<KIND, ORDER, T>;                 \
+  template <typename T> using Name##Bwd = BesselIntBwd<KIND, ORDER, T>;                 \
+  template <typename T> using Name##BwdBwd = BesselIntBwdBwd<KIND, ORDER, T>;
+TSB_BESSEL_INT_ALIASES(BesselJ1, kBJ, 1)
+TSB_BESSEL_INT_ALIASES(BesselY0, kBY, 0)
+TSB_BESSEL_INT_ALIASES(BesselY1, kBY, 1)
+TSB_BESSEL_INT_ALIASES(ModifiedBesselI0, kBI, 0)
+TSB_BESSEL_INT_ALIASES(ModifiedBesselI1, kBI, 1)
+TSB_BESSEL_INT_ALIASES(ModifiedBesselK0, kBK, 0)
+TSB_BESSEL_INT_ALIASES(ModifiedBesselK1, kBK, 1)
+#undef TSB_BESSEL_INT_ALIASES
+
+}  // namespace tsb

@@ -153,10 +153,69 @@ def beta(a: Tensor, b: Tensor) -> Tensor:
     return torch.ops.torchscience.beta(a, b)
 
 
+def bessel_j_1(z: Tensor) -> Tensor:
+    """Bessel function of the first kind of order one, J_1(z) (odd in z).
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_bessel_j_1.py).
+    """
+    return torch.ops.torchscience.bessel_j_1(z)
+
+
+def bessel_y_0(z: Tensor) -> Tensor:
+    """Bessel function of the second kind of order zero, Y_0(z); NaN for z < 0, -inf at 0.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_bessel_y_0.py).
+    """
+    return torch.ops.torchscience.bessel_y_0(z)
+
+
+def bessel_y_1(z: Tensor) -> Tensor:
+    """Bessel function of the second kind of order one, Y_1(z); NaN for z < 0, -inf at 0.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_bessel_y_1.py).
+    """
+    return torch.ops.torchscience.bessel_y_1(z)
+
+
+def modified_bessel_i_0(z: Tensor) -> Tensor:
+    """Modified Bessel function of the first kind of order zero, I_0(z) (even in z).
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_modified_bessel_i_0.py).
+    """
+    return torch.ops.torchscience.modified_bessel_i_0(z)
+
+
+def modified_bessel_i_1(z: Tensor) -> Tensor:
+    """Modified Bessel function of the first kind of order one, I_1(z) (odd in z).
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_modified_bessel_i_1.py).
+    """
+    return torch.ops.torchscience.modified_bessel_i_1(z)
+
+
+def modified_bessel_k_0(z: Tensor) -> Tensor:
+    """Modified Bessel function of the second kind of order zero, K_0(z); NaN for z < 0, +inf at 0.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_modified_bessel_k_0.py).
+    """
+    return torch.ops.torchscience.modified_bessel_k_0(z)
+
+
+def modified_bessel_k_1(z: Tensor) -> Tensor:
+    """Modified Bessel function of the second kind of order one, K_1(z); NaN for z < 0, +inf at 0.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_modified_bessel_k_1.py).
+    """
+    return torch.ops.torchscience.modified_bessel_k_1(z)
+
+
 __all__ = [
     "bessel_j",
     "bessel_j_0",
+    "bessel_j_1",
     "bessel_y",
+    "bessel_y_0",
+    "bessel_y_1",
     "beta",
     "complete_legendre_elliptic_integral_e",
     "complete_legendre_elliptic_integral_k",
@@ -166,7 +225,11 @@ __all__ = [
     "log_beta",
     "log_gamma",
     "modified_bessel_i",
+    "modified_bessel_i_0",
+    "modified_bessel_i_1",
     "modified_bessel_k",
+    "modified_bessel_k_0",
+    "modified_bessel_k_1",
     "polygamma",
     "regularized_gamma_p",
     "regularized_gamma_q",
