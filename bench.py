@@ -63,8 +63,9 @@ def make_inputs(seed: int, dtype=torch.float64):
 
 
 ELEMS = ROWS * COLS + STRESS
-# DRAM bytes (read 134.41 MB + write 8.97 MB) of one launch of the fused P backward on the grid, from ncu.
-TRAFFIC_BYTES_P_BWD = 142.78e6
+# DRAM bytes (read 0.20 MB + write 360.24 MB) of one launch of the fused P forward with derivatives on
+# the grid, from ncu (below the 402.7 MB written: the last tiles are still in L2 when the kernel ends).
+TRAFFIC_BYTES_P_FWDGRAD = 360.44e6
 
 
 # ------------------------------------------------------------------ clocks
@@ -173,31 +174,29 @@ def count_launches(fn) -> int:
 
 
 def kernel_roofline(dev_inputs, steps, flush):
-    """Times the dominant kernel (the fused broadcast-reduced FP64 backward over
-    the 4096 x 4096 grid) alone through the C ABI, on the launching stream."""
+    """Times the dominant kernel alone through the C ABI, on the launching
+    stream: the fused FP64 forward of autograd (P with dP/da and dP/dx in one
+    evaluation) over the 4096 x 4096 grid."""
     import ctypes
 
     from torchscience_b200._cabi import TsbTensor, describe, lib
 
-    a, x, g = dev_inputs[0], dev_inputs[1], dev_inputs[2]
-    ga = torch.empty_like(a)
-    gx = torch.empty_like(x)
+    a, x = dev_inputs[0], dev_inputs[1]
     shape = (ROWS, COLS)
-    din = (TsbTensor * 3)(describe(g, shape), describe(a, shape), describe(x, shape))
-    dout = (TsbTensor * 2)(describe(ga, shape), describe(gx, shape))
-    nb = lib().tsb_workspace_bytes(din, 3, dout, 2)
-    ws = torch.empty(max(nb, 1), dtype=torch.uint8, device=a.device)
+    outs = [torch.empty(shape, dtype=a.dtype, device=a.device) for _ in range(3)]
+    din = (TsbTensor * 2)(describe(a, shape), describe(x, shape))
+    dout = (TsbTensor * 3)(*[describe(t, shape) for t in outs])
     stream = torch.cuda.current_stream()
 
     def launch():
-        st = lib().tsb_regularized_gamma_p_backward(
-            din, 3, dout, 2, 0, ctypes.c_void_p(ws.data_ptr()), ctypes.c_int64(nb), ctypes.c_void_p(stream.cuda_stream)
+        st = lib().tsb_regularized_gamma_p_forward_with_grads(
+            din, 2, dout, 3, 0, None, ctypes.c_int64(0), ctypes.c_void_p(stream.cuda_stream)
         )
         assert st == 0, lib().tsb_last_error()
 
     sec = timed_steps(launch, steps, 2, flush) / steps
-    # algorithmic bytes: read g (8 B/elem) + a, x once + write the reduced grads
-    alg = ROWS * COLS * 8 + (ROWS + COLS) * 8 * 2
+    # algorithmic bytes: write P, dP/da, dP/dx (8 B/elem each) + read a, x once
+    alg = ROWS * COLS * 8 * 3 + (ROWS + COLS) * 8
     return sec, alg
 
 
@@ -291,16 +290,19 @@ def our_arm(args):
     gas_host = torch.empty(STRESS, dtype=torch.float64).pin_memory()
     gxs_host = torch.empty(STRESS, dtype=torch.float64).pin_memory()
 
-    # The step runs in row chunks on three streams, so that copying one chunk's
-    # upstream gradient in, evaluating another and copying a third's results
-    # out overlap (PCIe is full duplex).  Every chunk goes through the public
-    # API (special_functions + torch.autograd.grad); grad_x is the sum of the
-    # chunks' reduced gradients.
+    # The step runs in row chunks on three streams, so that copying the
+    # upstream gradient in, evaluating and copying results out overlap (PCIe
+    # is full duplex).  The forwards need only a and x, so they all run first
+    # and their outputs start back to the host while g is still arriving; each
+    # chunk's backward runs as its slice of g lands.  Every chunk goes through
+    # the public API (special_functions + torch.autograd.grad); grad_x is the
+    # sum of the chunks' reduced gradients.
     chunks = 8
     rows_c = ROWS // chunks
     s_in, s_comp, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     g_dev = torch.empty(ROWS, COLS, dtype=torch.float64, device=dev)
-    ev_in = [torch.cuda.Event() for _ in range(chunks + 1)]
+    ev_in = [torch.cuda.Event() for _ in range(chunks + 2)]
+    ev_y = [torch.cuda.Event() for _ in range(chunks + 1)]
     ev_out = [torch.cuda.Event() for _ in range(chunks + 1)]
 
     def e2e_step():
@@ -311,40 +313,54 @@ def our_arm(args):
         with torch.cuda.stream(s_in):
             a = a_h.to(dev, non_blocking=True)
             x = x_h.to(dev, non_blocking=True)
-            a_s, x_s, g_s = (t.to(dev, non_blocking=True) for t in (as_h, xs_h, gs_h))
+            a_s, x_s = as_h.to(dev, non_blocking=True), xs_h.to(dev, non_blocking=True)
+            ev_in[chunks].record(s_in)  # a, x and the stress arguments
             for i in range(chunks):
                 r = slice(i * rows_c, (i + 1) * rows_c)
                 g_dev[r].copy_(g_h[r], non_blocking=True)
                 ev_in[i].record(s_in)
+            g_s = gs_h.to(dev, non_blocking=True)
+            ev_in[chunks + 1].record(s_in)
         with torch.cuda.stream(s_comp):
-            xr = x.detach().requires_grad_(True)
-            gx = torch.zeros_like(x)
+            s_comp.wait_event(ev_in[chunks])
             for t in (a, x, a_s, x_s, g_s):
                 t.record_stream(s_comp)
+            xr = x.detach().requires_grad_(True)
+            asr, xsr = a_s.detach().requires_grad_(True), x_s.detach().requires_grad_(True)
+            ars, ys_ = [], []
+            for i in range(chunks + 1):
+                if i < chunks:
+                    ar = a[i * rows_c:(i + 1) * rows_c].detach().requires_grad_(True)
+                    y = sf.regularized_gamma_p(ar, xr)
+                    ars.append(ar)
+                else:
+                    y = sf.regularized_gamma_p(asr, xsr)
+                ys_.append(y)
+                ev_y[i].record(s_comp)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(ev_y[i])
+                    y.record_stream(s_out)
+                    dst = y_host[i * rows_c:(i + 1) * rows_c] if i < chunks else ys_host
+                    dst.copy_(y.detach(), non_blocking=True)
+            gx = torch.zeros_like(x)
             for i in range(chunks):
                 r = slice(i * rows_c, (i + 1) * rows_c)
                 s_comp.wait_event(ev_in[i])
-                ar = a[r].detach().requires_grad_(True)
-                y = sf.regularized_gamma_p(ar, xr)
-                ga, gxi = torch.autograd.grad(y, (ar, xr), g_dev[r])
+                ga, gxi = torch.autograd.grad(ys_[i], (ars[i], xr), g_dev[r])
                 gx += gxi
                 ev_out[i].record(s_comp)
                 with torch.cuda.stream(s_out):
                     s_out.wait_event(ev_out[i])
-                    for t in (y, ga):
-                        t.record_stream(s_out)
-                    y_host[r].copy_(y.detach(), non_blocking=True)
+                    ga.record_stream(s_out)
                     ga_host[r].copy_(ga, non_blocking=True)
-            asr, xsr = a_s.detach().requires_grad_(True), x_s.detach().requires_grad_(True)
-            ys = sf.regularized_gamma_p(asr, xsr)
-            gas, gxs = torch.autograd.grad(ys, (asr, xsr), g_s)
+            s_comp.wait_event(ev_in[chunks + 1])
+            gas, gxs = torch.autograd.grad(ys_[chunks], (asr, xsr), g_s)
             ev_out[chunks].record(s_comp)
         with torch.cuda.stream(s_out):
             s_out.wait_event(ev_out[chunks])
-            for t in (gx, ys, gas, gxs):
+            for t in (gx, gas, gxs):
                 t.record_stream(s_out)
             gx_host.copy_(gx, non_blocking=True)
-            ys_host.copy_(ys.detach(), non_blocking=True)
             gas_host.copy_(gas, non_blocking=True)
             gxs_host.copy_(gxs, non_blocking=True)
         main.wait_stream(s_out)
@@ -400,7 +416,8 @@ def our_arm(args):
         },
         "e2e": {
             "value": total / t_e2e / 1e9,
-            "pipeline": f"{chunks} row chunks over 3 streams (copy in / evaluate / copy out overlapped)",
+            "pipeline": f"{chunks} row chunks over 3 streams: forwards first (outputs copied out while g is copied in), "
+            "then each chunk's backward as its slice of g arrives",
             "check_vs_device_step": e2e_check,
             "unit": "Gelem/s",
             "h2d_bytes_per_step": h2d,
@@ -418,7 +435,8 @@ def our_arm(args):
             pass
     achieved = k_bytes / k_sec / 1e9
     result["roofline"] = {
-        "kernel": "reduce2d_kernel<IgammaBwd<double>> (fused broadcast-reduced FP64 backward, 4096x4096)",
+        "kernel": "reduce2d_kernel<IgammaFwdGrad<double>> (autograd's fused FP64 forward: P, dP/da, dP/dx, "
+        "4096x4096)",
         "bound": "hbm",
         "achieved": achieved,
         "peak": peak,
@@ -426,8 +444,8 @@ def our_arm(args):
         "unit": "GB/s",
         "frac": achieved / peak,
         # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel on this
-        # workload (ncu capture summarised in profiles/igamma_p_bwd_reduce2d_4096x4096_fp64.md)
-        "traffic": TRAFFIC_BYTES_P_BWD,
+        # workload (ncu capture summarised in profiles/igamma_p_fwdgrad_reduce2d_4096x4096_fp64.md)
+        "traffic": TRAFFIC_BYTES_P_FWDGRAD,
         "kernel_ms": k_sec * 1e3,
         "algorithmic_bytes_per_launch": k_bytes,
         "note": "compute-bound (FP64 pipe); the HBM fraction is small by construction; FP64-pipe utilisation "

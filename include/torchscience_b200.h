@@ -230,6 +230,18 @@ TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1);
 TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1_backward);
 TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1_backward_backward);
 
+/* ---- Fused forward for autograd (no counterpart in the reference) -------- */
+/* regularized_gamma_p / _q with their first derivatives in one evaluation: in = {a, x}, out =
+ * {P (Q), d/da, d/dx} at the broadcast shape; a NULL d/da output is skipped.  The autograd forward of
+ * regularized_gamma_p/_q uses it when an input requires grad and keeps the derivatives, so the backward
+ * is tsb_gradient_product instead of a second evaluation (the reference's autograd calls
+ * regularized_gamma_p and later regularized_gamma_p_backward, autograd/special_functions.h:15). */
+TSB_OP_SIGNATURE(tsb_regularized_gamma_p_forward_with_grads);
+TSB_OP_SIGNATURE(tsb_regularized_gamma_q_forward_with_grads);
+/* in = {grad, d_a, d_b}, out = {grad*d_a, grad*d_b}, each reduced (summed) to its output's shape when
+ * that output broadcasts, like the reduced backward entry points. */
+TSB_OP_SIGNATURE(tsb_gradient_product);
+
 /* ---- Probability callers of the incomplete gamma ----------------------- */
 /* gamma_cumulative_distribution(x, shape, scale): kernel/probability/gamma_cumulative_distribution.h:9-13,
  * schema torchscience.cpp:1909-1910; backward gamma_cumulative_distribution_backward.h:16-43

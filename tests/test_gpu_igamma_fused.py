@@ -1,0 +1,110 @@
+"""The autograd path of regularized_gamma_p / _q when an input requires grad:
+the forward evaluates P (Q) with its first derivatives in one pass and keeps
+them, the backward multiplies them by the incoming gradient and reduces.  Its
+gradients must equal the reference-named backward op's (which evaluates again
+from the inputs), its forward value the plain forward's, and double backward
+must keep working."""
+
+import pytest
+import torch
+
+import torchscience_b200  # noqa: F401
+from torchscience_b200 import special_functions as sf
+
+pytestmark = pytest.mark.gpu
+
+OPS = {"p": sf.regularized_gamma_p, "q": sf.regularized_gamma_q}
+
+
+def inputs(shape_a, shape_x, dtype=torch.float64, seed=0):
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    a = torch.exp(torch.rand(shape_a, device="cuda", dtype=torch.float64, generator=gen) * 11.5 - 4.6).to(dtype)
+    x = torch.exp(torch.rand(shape_x, device="cuda", dtype=torch.float64, generator=gen) * 14.5 - 6.9).to(dtype)
+    return a, x
+
+
+def close(got, want, terms, tol):
+    """|got - want| <= tol x (the sum of |terms| behind each reduced entry).
+    `want` and `terms` are the backward op's full-shape gradients (the
+    reference's _backward ops return them unreduced), summed to got's shape."""
+    want, terms = want.double().sum_to_size(got.shape), terms.double().abs().sum_to_size(got.shape)
+    return bool(((got.double() - want).abs() <= tol * terms + 1e-300).all())
+
+
+@pytest.mark.parametrize("which", ["p", "q"])
+@pytest.mark.parametrize("layout", ["grid", "contiguous"])
+def test_fused_gradients_equal_the_backward_op(which, layout):
+    fn = OPS[which]
+    if layout == "grid":
+        a, x = inputs((384, 1), (1, 448))
+    else:
+        a, x = inputs((50000,), (50000,), seed=1)
+        x = a * (1 + (x / x.max() - 0.5) * 2e-2)  # |x - a| < 1e-2 a, the benchmark's stress set
+    g = torch.randn(torch.broadcast_shapes(a.shape, x.shape), device="cuda", dtype=torch.float64)
+    ar, xr = a.clone().requires_grad_(True), x.clone().requires_grad_(True)
+    y = fn(ar, xr)
+    ga, gx = torch.autograd.grad(y, (ar, xr), g)
+    with torch.no_grad():
+        y0 = fn(a, x)
+        ra, rx = getattr(torch.ops.torchscience, f"regularized_gamma_{which}_backward")(g, a, x)
+        # per-entry scale of the reduction: the same reduction of |g·dP|
+        ta, tx = getattr(torch.ops.torchscience, f"regularized_gamma_{which}_backward")(g.abs(), a, x)
+    # the value comes from the derivative-carrying series / fraction, which may stop
+    # a term later: equal to the plain forward within the evaluator's accuracy
+    bound = 16 * 2.2e-16 * (1 + y0.abs().clamp_min(1e-300).log().abs()) * y0.abs()
+    assert bool(((y - y0).abs() <= bound).all())
+    assert close(ga, ra, ta, 1e-13) and close(gx, rx, tx, 1e-13)
+
+
+@pytest.mark.parametrize("wants", ["a", "x"])
+def test_one_input_requires_grad(wants):
+    a, x = inputs((256, 1), (1, 320), seed=2)
+    g = torch.randn(256, 320, device="cuda", dtype=torch.float64)
+    ar = a.clone().requires_grad_(wants == "a")
+    xr = x.clone().requires_grad_(wants == "x")
+    y = sf.regularized_gamma_p(ar, xr)
+    (gr,) = torch.autograd.grad(y, (ar if wants == "a" else xr,), g)
+    with torch.no_grad():
+        ra, rx = torch.ops.torchscience.regularized_gamma_p_backward(g, a, x)
+        ta, tx = torch.ops.torchscience.regularized_gamma_p_backward(g.abs(), a, x)
+    want, terms = (ra, ta) if wants == "a" else (rx, tx)
+    assert close(gr, want, terms, 1e-13)
+
+
+def test_float32_data():
+    a, x = inputs((256, 1), (1, 320), dtype=torch.float32, seed=3)
+    g = torch.randn(256, 320, device="cuda", dtype=torch.float32)
+    ar, xr = a.clone().requires_grad_(True), x.clone().requires_grad_(True)
+    ga, gx = torch.autograd.grad(sf.regularized_gamma_p(ar, xr), (ar, xr), g)
+    with torch.no_grad():
+        ra, rx = torch.ops.torchscience.regularized_gamma_p_backward(g, a, x)
+        ta, tx = torch.ops.torchscience.regularized_gamma_p_backward(g.abs(), a, x)
+    assert close(ga, ra, ta, 2e-6) and close(gx, rx, tx, 2e-6)
+
+
+def test_double_backward_through_the_fused_path():
+    gen = torch.Generator(device="cuda").manual_seed(4)
+    a = (torch.rand(5, 1, device="cuda", dtype=torch.float64, generator=gen) * 5 + 0.3).requires_grad_()
+    x = (torch.rand(1, 4, device="cuda", dtype=torch.float64, generator=gen) * 6 + 0.2).requires_grad_()
+    for fn in OPS.values():
+        assert torch.autograd.gradcheck(fn, (a, x), eps=1e-6, atol=1e-7, rtol=1e-5)
+        assert torch.autograd.gradgradcheck(fn, (a, x), eps=1e-6, atol=1e-6, rtol=1e-4)
+
+
+def test_derivatives_are_kept_only_for_a_recorded_forward():
+    """With grad enabled the forward keeps dP/da and dP/dx (two more tensors
+    of the output's size stay alive with the graph); under no_grad the plain
+    forward runs and only the output exists."""
+    a, x = inputs((1024, 1), (1, 1024), seed=5)
+    ar, xr = a.clone().requires_grad_(True), x.clone().requires_grad_(True)
+    size = 1024 * 1024 * 8
+    torch.cuda.synchronize()
+    m0 = torch.cuda.memory_allocated()
+    y = sf.regularized_gamma_p(ar, xr)
+    kept = torch.cuda.memory_allocated() - m0
+    del y
+    with torch.no_grad():
+        m1 = torch.cuda.memory_allocated()
+        y = sf.regularized_gamma_p(ar, xr)
+        plain = torch.cuda.memory_allocated() - m1
+    assert kept >= 3 * size and plain < 2 * size

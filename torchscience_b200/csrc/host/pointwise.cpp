@@ -145,6 +145,11 @@ std::vector<at::Tensor> run_reduced_backward(OpFn fn, const char* name, const at
   std::vector<at::Tensor> all;
   all.push_back(grad);
   for (const auto& t : fwd_inputs) all.push_back(t);
+  return run_reduced(fn, name, all, fwd_inputs, want);
+}
+
+std::vector<at::Tensor> run_reduced(OpFn fn, const char* name, at::TensorList all, at::TensorList fwd_inputs,
+                                    const std::vector<bool>& want) {
   const at::ScalarType dt = checked_common_dtype(name, all);
   const at::Device dev = checked_device(name, all);
   c10::cuda::CUDAGuard guard(dev);
@@ -205,6 +210,36 @@ std::vector<at::Tensor> run_reduced_backward(OpFn fn, const char* name, const at
                   ws > 0 ? workspace.data_ptr() : nullptr, ws, stream),
                name);
   return grads;
+}
+
+std::vector<at::Tensor> run_pointwise_masked(OpFn fn, const char* name, at::TensorList inputs, int n_out,
+                                             const std::vector<bool>& want) {
+  const at::ScalarType dt = checked_common_dtype(name, inputs);
+  const at::Device dev = checked_device(name, inputs);
+  c10::cuda::CUDAGuard guard(dev);
+  std::vector<at::Tensor> ins = prepare_inputs(inputs, dt, dev);
+  at::DimVector full(ins[0].sizes().begin(), ins[0].sizes().end());
+  for (size_t i = 1; i < ins.size(); ++i) full = at::infer_size_dimvector(full, ins[i].sizes());
+  const auto opts = ins[0].options();
+  std::vector<at::Tensor> res(n_out);
+  for (int o = 0; o < n_out; ++o)
+    if (want[o]) res[o] = at::empty(full, opts);
+  int64_t numel = 1;
+  for (auto v : full) numel *= v;
+  if (numel == 0) return res;
+  if (full.size() > TSB_MAX_DIMS) {  // every output through run_pointwise, unwanted ones dropped
+    auto all = run_pointwise(fn, name, ins, n_out);
+    for (int o = 0; o < n_out; ++o)
+      if (want[o]) res[o] = all[o];
+    return res;
+  }
+  std::vector<tsb_tensor> din, dout;
+  for (const auto& t : ins) din.push_back(describe(t, full));
+  for (int o = 0; o < n_out; ++o) dout.push_back(want[o] ? describe(res[o], full) : describe(at::Tensor(), full, false));
+  const auto stream = c10::cuda::getCurrentCUDAStream(dev.index()).stream();
+  check_status(fn(din.data(), (int32_t)din.size(), dout.data(), n_out, precision_mode().load(), nullptr, 0, stream),
+               name);
+  return res;
 }
 
 std::vector<at::Tensor> meta_pointwise(const char* name, at::TensorList inputs, int n_out) {

@@ -44,6 +44,16 @@ std::vector<at::Tensor> run_pointwise(OpFn fn, const char* name, at::TensorList 
 std::vector<at::Tensor> run_reduced_backward(OpFn fn, const char* name, const at::Tensor& grad,
                                              at::TensorList fwd_inputs, const std::vector<bool>& want);
 
+// run_pointwise computing only the outputs with want[o] set (the others come
+// back undefined; the kernel skips them).
+std::vector<at::Tensor> run_pointwise_masked(OpFn fn, const char* name, at::TensorList inputs, int n_out,
+                                             const std::vector<bool>& want);
+
+// General form of run_reduced_backward: `kernel_inputs` go to the kernel as
+// they are (broadcast together), output i is reduced to out_like[i]'s shape.
+std::vector<at::Tensor> run_reduced(OpFn fn, const char* name, at::TensorList kernel_inputs, at::TensorList out_like,
+                                    const std::vector<bool>& want);
+
 // Meta (shape/dtype only) version of run_pointwise.
 std::vector<at::Tensor> meta_pointwise(const char* name, at::TensorList inputs, int n_out);
 

@@ -141,7 +141,7 @@ inline torch::autograd::variable_list defined_or_zero(std::vector<at::Tensor> r,
   TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl(#name, tsbh::ops::name##_autocast); }
 
 // --------------------------------------------------------------- binary ops
-#define TSBH_BINARY_OP(name, Cls, A, B, FWD, BWD, BB)                                                   \
+#define TSBH_BINARY_OP_CORE(name, Cls, A, B, FWD, BWD, BB)                                                   \
   namespace tsbh::ops {                                                                                 \
   at::Tensor name##_cuda(const at::Tensor& a, const at::Tensor& b) {                                   \
     return run_pointwise(FWD, #name, {a, b}, 1)[0];                                                    \
@@ -258,8 +258,92 @@ inline torch::autograd::variable_list defined_or_zero(std::vector<at::Tensor> r,
     m.impl(#name "_backward", tsbh::ops::name##_backward_cpu);                                          \
     m.impl(#name "_backward_backward", tsbh::ops::name##_backward_backward_cpu);                        \
   }                                                                                                     \
-  TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl(#name, tsbh::ops::name##_autograd); }         \
   TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl(#name, tsbh::ops::name##_autocast); }
+#define TSBH_BINARY_OP(name, Cls, A, B, FWD, BWD, BB)     \
+  TSBH_BINARY_OP_CORE(name, Cls, A, B, FWD, BWD, BB)      \
+  TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl(#name, tsbh::ops::name##_autograd); }
+
+// Autograd for P and Q: when an input requires grad on CUDA, the forward runs
+// the fused kernel (value and first derivatives in one evaluation) and keeps
+// the derivatives; the backward multiplies them by the incoming gradient and
+// reduces to the inputs' shapes (an HBM-bound pass instead of a second
+// evaluation).  Double backward is unchanged: the _backward_backward op from
+// the saved inputs.  Without grad (no input requiring it, or grad mode off),
+// or off CUDA, the plain forward runs.
+#define TSBH_IGAMMA_FUSED_AUTOGRAD(name, Cls, FWDGRAD)                                                           \
+  namespace tsbh::ops {                                                                                          \
+  class Cls##SavedBackward : public torch::autograd::Function<Cls##SavedBackward> {                              \
+   public:                                                                                                       \
+    static variable_list forward(AutogradContext* ctx, const at::Tensor& g, const at::Tensor& a,                \
+                                 const at::Tensor& b, const at::Tensor& da, const at::Tensor& db, bool ra,      \
+                                 bool rb) {                                                                      \
+      ctx->save_for_backward({g, a, b});                                                                        \
+      ctx->saved_data["ra"] = ra;                                                                               \
+      ctx->saved_data["rb"] = rb;                                                                               \
+      at::AutoDispatchBelowAutograd guard;                                                                      \
+      return defined_or_zero(run_reduced(tsb_gradient_product, #name "_backward", {g, da, db}, {a, b}, {ra, rb}), \
+                             {a, b});                                                                           \
+    }                                                                                                            \
+    static variable_list backward(AutogradContext* ctx, const variable_list& go) {                              \
+      auto saved = ctx->get_saved_variables();                                                                   \
+      const bool ra = ctx->saved_data["ra"].toBool(), rb = ctx->saved_data["rb"].toBool();                      \
+      const at::Tensor none;                                                                                     \
+      if ((!go[0].defined() && !go[1].defined()) || (!ra && !rb)) return {none, none, none, none, none, none, none}; \
+      at::AutoDispatchBelowAutograd guard;                                                                      \
+      auto gga = go[0].defined() ? go[0] : at::zeros_like(saved[1]);                                            \
+      auto ggb = go[1].defined() ? go[1] : at::zeros_like(saved[2]);                                            \
+      static auto op = c10::Dispatcher::singleton()                                                             \
+                           .findSchemaOrThrow("torchscience::" #name "_backward_backward", "")                  \
+                           .typed<std::tuple<at::Tensor, at::Tensor, at::Tensor>(                               \
+                               const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,      \
+                               const at::Tensor&)>();                                                           \
+      auto [gg_out, g_a, g_b] = op.call(gga, ggb, saved[0], saved[1], saved[2]);                                \
+      return {gg_out, g_a, g_b, none, none, none, none};                                                        \
+    }                                                                                                            \
+  };                                                                                                             \
+  class Cls##Fused : public torch::autograd::Function<Cls##Fused> {                                              \
+   public:                                                                                                       \
+    static at::Tensor forward(AutogradContext* ctx, const at::Tensor& a, const at::Tensor& b, bool recorded) {  \
+      const bool ra = wants_grad(a), rb = wants_grad(b);                                                        \
+      ctx->saved_data["ra"] = ra;                                                                               \
+      ctx->saved_data["rb"] = rb;                                                                               \
+      at::AutoDispatchBelowAutograd guard;                                                                      \
+      if ((ra || rb) && recorded && any_cuda({a, b})) {                                                         \
+        auto r = run_pointwise_masked(FWDGRAD, #name, {a, b}, 3, {true, ra, rb});                               \
+        ctx->save_for_backward({a, b, r[1], r[2]});                                                             \
+        ctx->saved_data["fused"] = true;                                                                        \
+        return r[0];                                                                                             \
+      }                                                                                                          \
+      ctx->save_for_backward({a, b});                                                                           \
+      ctx->saved_data["fused"] = false;                                                                         \
+      static auto op = c10::Dispatcher::singleton()                                                             \
+                           .findSchemaOrThrow("torchscience::" #name, "")                                       \
+                           .typed<at::Tensor(const at::Tensor&, const at::Tensor&)>();                          \
+      return op.call(a, b);                                                                                      \
+    }                                                                                                            \
+    static variable_list backward(AutogradContext* ctx, const variable_list& go) {                              \
+      auto saved = ctx->get_saved_variables();                                                                   \
+      const bool ra = ctx->saved_data["ra"].toBool(), rb = ctx->saved_data["rb"].toBool();                      \
+      if (!go[0].defined()) return {at::Tensor(), at::Tensor(), at::Tensor()};                                  \
+      if (!ctx->saved_data["fused"].toBool()) {                                                                 \
+        auto g = Cls##Backward::apply(go[0], saved[0], saved[1], ra, rb);                                        \
+        return {ra ? g[0] : at::Tensor(), rb ? g[1] : at::Tensor(), at::Tensor()};                              \
+      }                                                                                                          \
+      /* an unwanted derivative was not kept: the other stands in (autograd Functions take no undefined      */ \
+      /* tensors), and its product is skipped                                                                 */ \
+      const at::Tensor& d0 = saved[2].defined() ? saved[2] : saved[3];                                           \
+      const at::Tensor& d1 = saved[3].defined() ? saved[3] : saved[2];                                           \
+      auto g = Cls##SavedBackward::apply(go[0], saved[0], saved[1], d0, d1, ra, rb);                             \
+      return {ra ? g[0] : at::Tensor(), rb ? g[1] : at::Tensor(), at::Tensor()};                                \
+    }                                                                                                            \
+  };                                                                                                             \
+  /* under no_grad the autograd kernel still runs, and apply() turns grad mode off before forward(): */           \
+  /* whether this call is recorded is read here                                                       */           \
+  at::Tensor name##_fused_autograd(const at::Tensor& a, const at::Tensor& b) {                                  \
+    return Cls##Fused::apply(a, b, c10::GradMode::is_enabled());                                                \
+  }                                                                                                              \
+  } /* namespace tsbh::ops */                                                                                    \
+  TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl(#name, tsbh::ops::name##_fused_autograd); }
 
 // Schemas: identical strings to the reference's TORCH_LIBRARY block.
 TORCH_LIBRARY(torchscience, m) { TSB_DEFINE_TORCHSCIENCE_SCHEMAS(m) }
@@ -268,10 +352,12 @@ TSBH_UNARY_OP(log_gamma, LogGamma, z, tsb_log_gamma, tsb_log_gamma_backward, tsb
 TSBH_UNARY_OP(gamma, Gamma, z, tsb_gamma, tsb_gamma_backward, tsb_gamma_backward_backward)
 TSBH_UNARY_OP(digamma, Digamma, z, tsb_digamma, tsb_digamma_backward, tsb_digamma_backward_backward)
 TSBH_UNARY_OP(trigamma, Trigamma, z, tsb_trigamma, tsb_trigamma_backward, tsb_trigamma_backward_backward)
-TSBH_BINARY_OP(regularized_gamma_p, RegularizedGammaP, a, x, tsb_regularized_gamma_p, tsb_regularized_gamma_p_backward,
-               tsb_regularized_gamma_p_backward_backward)
-TSBH_BINARY_OP(regularized_gamma_q, RegularizedGammaQ, a, x, tsb_regularized_gamma_q, tsb_regularized_gamma_q_backward,
-               tsb_regularized_gamma_q_backward_backward)
+TSBH_BINARY_OP_CORE(regularized_gamma_p, RegularizedGammaP, a, x, tsb_regularized_gamma_p,
+                    tsb_regularized_gamma_p_backward, tsb_regularized_gamma_p_backward_backward)
+TSBH_IGAMMA_FUSED_AUTOGRAD(regularized_gamma_p, RegularizedGammaP, tsb_regularized_gamma_p_forward_with_grads)
+TSBH_BINARY_OP_CORE(regularized_gamma_q, RegularizedGammaQ, a, x, tsb_regularized_gamma_q,
+                    tsb_regularized_gamma_q_backward, tsb_regularized_gamma_q_backward_backward)
+TSBH_IGAMMA_FUSED_AUTOGRAD(regularized_gamma_q, RegularizedGammaQ, tsb_regularized_gamma_q_forward_with_grads)
 TSBH_BINARY_OP(polygamma, Polygamma, n, z, tsb_polygamma, tsb_polygamma_backward, tsb_polygamma_backward_backward)
 TSBH_BINARY_OP(log_beta, LogBeta, a, b, tsb_log_beta, tsb_log_beta_backward, tsb_log_beta_backward_backward)
 TSBH_BINARY_OP(beta, Beta, a, b, tsb_beta, tsb_beta_backward, tsb_beta_backward_backward)

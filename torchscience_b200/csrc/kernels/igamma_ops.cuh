@@ -98,11 +98,61 @@ struct IgammaBwdBwd : IgammaAuxIO<2, 3, 4, T_> {
   }
 };
 
+// Forward with the first derivatives, for autograd: in = {a, x}, out =
+// {P (or Q), ∂/∂a, ∂/∂x} at full shape, in one evaluation.  A training step
+// that differentiates P otherwise evaluates the series or fraction twice, once
+// for the value and again in the backward; here the backward only multiplies
+// the kept derivatives by its incoming gradient (GradProduct).  ∂/∂a is
+// skipped when its output is not requested (then ∂/∂x alone, as in the
+// backward above).
+#ifndef TSB_IGFG_TR
+#define TSB_IGFG_TR 64
+#endif
+template <typename T_, bool UPPER>
+struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 3, R = kIgRegions;
+  static constexpr int MIN_BLOCKS = 4;
+  static constexpr int TILE_ROWS = TSB_IGFG_TR;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int r, const T* in, T* out, uint32_t mask, const double* A = nullptr,
+                              const double* X = nullptr) {
+    const double sgn = UPPER ? -1.0 : 1.0;
+    const IgPre P = IgammaFwdGrad::pre(in, A, X);
+    if (!(mask & 2u)) {
+      const IgammaOut o = igamma_eval<0, UPPER>(r, (double)in[0], (double)in[1], P);
+      out[0] = (T)(UPPER ? o.q : o.p);
+      out[1] = T(0);
+      out[2] = (T)(sgn * igamma_px_only((double)in[0], (double)in[1], P));
+      return;
+    }
+    const IgammaOut o = igamma_eval<1, UPPER>(r, (double)in[0], (double)in[1], P);
+    out[0] = (T)(UPPER ? o.q : o.p);
+    out[1] = (T)(sgn * o.pa);
+    out[2] = (T)(sgn * o.px);
+  }
+};
+
+// Backward from kept derivatives: in = {grad, d_a, d_b}, out = {grad·d_a,
+// grad·d_b}, each reduced to its input's shape by the 2-D kernel.
+template <typename T_>
+struct GradProduct {
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    out[0] = in[0] * in[1];
+    out[1] = in[0] * in[2];
+  }
+};
+
 template <typename T> using GammaPFwd = IgammaFwd<T, false>;
 template <typename T> using GammaPBwd = IgammaBwd<T, false>;
 template <typename T> using GammaPBwdBwd = IgammaBwdBwd<T, false>;
 template <typename T> using GammaQFwd = IgammaFwd<T, true>;
 template <typename T> using GammaQBwd = IgammaBwd<T, true>;
 template <typename T> using GammaQBwdBwd = IgammaBwdBwd<T, true>;
+template <typename T> using GammaPFwdGrad = IgammaFwdGrad<T, false>;
+template <typename T> using GammaQFwdGrad = IgammaFwdGrad<T, true>;
 
 }  // namespace tsb

@@ -234,6 +234,17 @@ struct MinBlocks<Fn, decltype((void)Fn::MIN_BLOCKS, void())> {
   static constexpr int value = Fn::MIN_BLOCKS;
 };
 
+// Rows of a 2-D tile: a functor's TILE_ROWS (32 or 64) if it sets one, else
+// 64 when the staging fits in 64 KB and 32 otherwise.
+template <class Fn, class = void>
+struct TileRows {
+  static constexpr int value = 0;
+};
+template <class Fn>
+struct TileRows<Fn, decltype((void)Fn::TILE_ROWS, void())> {
+  static constexpr int value = Fn::TILE_ROWS;
+};
+
 template <class Fn, class = void>
 struct HasAuxIdx {
   static constexpr int i0 = -1, i1 = -1;
@@ -407,8 +418,13 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<Fn>::value) map_kernel(const
 template <class Fn>
 struct ReduceTile {
   static constexpr int NSTAGED = HasAux<Fn>::value ? Fn::NIN - 2 : Fn::NIN;
-  static constexpr int NBUF = NSTAGED > Fn::NOUT ? NSTAGED : Fn::NOUT;
-  static constexpr int TR = Stage<Fn, 64 * kTC, NBUF>::SMEM <= 64 * 1024 ? 64 : kTRMin;
+  // A single-region functor without tables is evaluated as its inputs are
+  // loaded: only its outputs are staged (for the reductions and the stores).
+  static constexpr bool EVAL_ON_LOAD = !HasAux<Fn>::value && Fn::R == 1;
+  static constexpr int NBUF = EVAL_ON_LOAD ? Fn::NOUT : (NSTAGED > Fn::NOUT ? NSTAGED : Fn::NOUT);
+  static constexpr int TR = TileRows<Fn>::value ? TileRows<Fn>::value
+                                                : (Stage<Fn, 64 * kTC, NBUF>::SMEM <= 64 * 1024 ? 64 : kTRMin);
+  static_assert(TR == 32 || TR == 64, "2-D tiles are 32 or 64 rows");
   using S = Stage<Fn, TR * kTC, NBUF>;
   // staging slot of input q (-1: a table input)
   __host__ __device__ static constexpr int slot(int q) {
@@ -489,12 +505,19 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<Fn>::value) reduce2d_kernel(
 #pragma unroll
         for (int q = 0; q < NIN; ++q)
           v[q] = load_as<TS, T>(p.in_ptr[q] + (r * p.in_s0[q] + c * p.in_s1[q]) * (int64_t)sizeof(TS));
-        if constexpr (AUX) reg[k] = Fn::classify(v, aux_at<N0>(s_aux0, mode0, li), aux_at<N1>(s_aux1, mode1, li));
-        else if constexpr (R > 1) reg[k] = Fn::classify(v);
-        else reg[k] = 0;
+        if constexpr (RT::EVAL_ON_LOAD) {
+          T o[NOUT];
+          Fn::eval(0, v, o, p.out_mask);
 #pragma unroll
-        for (int q = 0; q < NIN; ++q)
-          if (RT::slot(q) >= 0) buf[RT::slot(q) * TILE + li] = v[q];
+          for (int q = 0; q < NOUT; ++q) buf[q * TILE + li] = o[q];
+        } else {
+          if constexpr (AUX) reg[k] = Fn::classify(v, aux_at<N0>(s_aux0, mode0, li), aux_at<N1>(s_aux1, mode1, li));
+          else if constexpr (R > 1) reg[k] = Fn::classify(v);
+          else reg[k] = 0;
+#pragma unroll
+          for (int q = 0; q < NIN; ++q)
+            if (RT::slot(q) >= 0) buf[RT::slot(q) * TILE + li] = v[q];
+        }
       }
     }
     if constexpr (AUX) {
@@ -533,19 +556,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<Fn>::value) reduce2d_kernel(
       const int count = cta_sort_by_region<R, EPT>(reg, list, regs, s_cnt, s_base, &s_next);
       cta_eval_groups<Fn, TILE, false>(count, buf, list, regs, p.out_mask, &s_next, nullptr, 0, nullptr, 0);
     } else {
-#pragma unroll
-      for (int k = 0; k < EPT; ++k) {
-        const int li = k * kBlock + tid;
-        if (reg[k] < R) {
-          T v[NIN], o[NOUT];
-#pragma unroll
-          for (int q = 0; q < NIN; ++q) v[q] = buf[q * TILE + li];
-          Fn::eval(0, v, o, p.out_mask);
-#pragma unroll
-          for (int q = 0; q < NOUT; ++q) buf[q * TILE + li] = o[q];
-        }
-      }
-      __syncthreads();
+      __syncthreads();  // single region: evaluated on load
     }
 
     const int rows_here = (int)(p.rows - r0 < (int64_t)TR ? p.rows - r0 : (int64_t)TR);
