@@ -230,6 +230,40 @@ TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1);
 TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1_backward);
 TSB_OP_SIGNATURE(tsb_hypergeometric_2_f_1_backward_backward);
 
+/* ---- Spherical Bessel functions of order 0 and 1 (unary) ------------------ */
+/* spherical_bessel_j_0(z): kernel/special_functions/spherical_bessel_j_0.h:33-44, schema torchscience.cpp:922-924. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j_0);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j_0_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j_0_backward_backward);
+/* spherical_bessel_j_1(z): kernel/special_functions/spherical_bessel_j_1.h:33-45, schema torchscience.cpp:927-929. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j_1);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j_1_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j_1_backward_backward);
+/* spherical_bessel_y_0(z): kernel/special_functions/spherical_bessel_y_0.h:33-41, schema torchscience.cpp:937-939. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y_0);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y_0_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y_0_backward_backward);
+/* spherical_bessel_y_1(z): kernel/special_functions/spherical_bessel_y_1.h:33-42, schema torchscience.cpp:942-944. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y_1);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y_1_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y_1_backward_backward);
+/* spherical_bessel_i_0(z): kernel/special_functions/spherical_bessel_i_0.h:33-47, schema torchscience.cpp:952-954. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i_0);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i_0_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i_0_backward_backward);
+/* spherical_bessel_i_1(z): kernel/special_functions/spherical_bessel_i_1.h:33-45, schema torchscience.cpp:957-959. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i_1);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i_1_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i_1_backward_backward);
+/* spherical_bessel_k_0(z): kernel/special_functions/spherical_bessel_k_0.h:33-49, schema torchscience.cpp:967-969. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k_0);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k_0_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k_0_backward_backward);
+/* spherical_bessel_k_1(z): kernel/special_functions/spherical_bessel_k_1.h:33-46, schema torchscience.cpp:972-974. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k_1);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k_1_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k_1_backward_backward);
+
 /* ---- Fused forward for autograd (no counterpart in the reference) -------- */
 /* regularized_gamma_p / _q with their first derivatives in one evaluation: in = {a, x}, out =
  * {P (Q), d/da, d/dx} at the broadcast shape; a NULL d/da output is skipped.  The autograd forward of

@@ -57,6 +57,30 @@
 #include "kernel/special_functions/modified_bessel_k_1.h"
 #include "kernel/special_functions/modified_bessel_k_1_backward.h"
 #include "kernel/special_functions/modified_bessel_k_1_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_j_0.h"
+#include "kernel/special_functions/spherical_bessel_j_0_backward.h"
+#include "kernel/special_functions/spherical_bessel_j_0_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_j_1.h"
+#include "kernel/special_functions/spherical_bessel_j_1_backward.h"
+#include "kernel/special_functions/spherical_bessel_j_1_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_y_0.h"
+#include "kernel/special_functions/spherical_bessel_y_0_backward.h"
+#include "kernel/special_functions/spherical_bessel_y_0_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_y_1.h"
+#include "kernel/special_functions/spherical_bessel_y_1_backward.h"
+#include "kernel/special_functions/spherical_bessel_y_1_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_i_0.h"
+#include "kernel/special_functions/spherical_bessel_i_0_backward.h"
+#include "kernel/special_functions/spherical_bessel_i_0_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_i_1.h"
+#include "kernel/special_functions/spherical_bessel_i_1_backward.h"
+#include "kernel/special_functions/spherical_bessel_i_1_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_k_0.h"
+#include "kernel/special_functions/spherical_bessel_k_0_backward.h"
+#include "kernel/special_functions/spherical_bessel_k_0_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_k_1.h"
+#include "kernel/special_functions/spherical_bessel_k_1_backward.h"
+#include "kernel/special_functions/spherical_bessel_k_1_backward_backward.h"
 #include "kernel/special_functions/bessel_j.h"
 #include "kernel/special_functions/bessel_j_0.h"
 #include "kernel/special_functions/bessel_j_0_backward.h"
@@ -177,6 +201,14 @@ static int eval_typed(const char* name, int pass, const void* const* in, void* c
   UNARY(digamma)
   UNARY(trigamma)
   UNARY(bessel_j_0)
+  UNARY(spherical_bessel_j_0)
+  UNARY(spherical_bessel_j_1)
+  UNARY(spherical_bessel_y_0)
+  UNARY(spherical_bessel_y_1)
+  UNARY(spherical_bessel_i_0)
+  UNARY(spherical_bessel_i_1)
+  UNARY(spherical_bessel_k_0)
+  UNARY(spherical_bessel_k_1)
   UNARY(bessel_j_1)
   UNARY(bessel_y_0)
   UNARY(bessel_y_1)

@@ -503,8 +503,51 @@ def bessel_int():
     np.savez_compressed(OUT / "bessel_int.npz", **d)
 
 
+SPH01 = {  # closed forms at 50 digits
+    "spherical_bessel_j_0": lambda z: mp.sin(z) / z, "spherical_bessel_j_1": lambda z: mp.sin(z) / z**2 - mp.cos(z) / z,
+    "spherical_bessel_y_0": lambda z: -mp.cos(z) / z,
+    "spherical_bessel_y_1": lambda z: -mp.cos(z) / z**2 - mp.sin(z) / z,
+    "spherical_bessel_i_0": lambda z: mp.sinh(z) / z,
+    "spherical_bessel_i_1": lambda z: mp.cosh(z) / z - mp.sinh(z) / z**2,
+    "spherical_bessel_k_0": lambda z: mp.pi / 2 * mp.exp(-z) / z,
+    "spherical_bessel_k_1": lambda z: mp.pi / 2 * (1 + z) * mp.exp(-z) / z**2}
+
+
+def spherical01():
+    """Spherical Bessel functions of order 0 and 1: z uniform in [-30, 30],
+    log-uniform magnitudes in [1e-8, 600] of both signs (k: [1e-8, 600]),
+    points within relative 1e-10..1e-4 of the first zeros of j0, j1, y0, y1;
+    values, first and second derivatives from the closed forms at 50 digits
+    (mpmath); the reference's forward, backward and double backward outputs;
+    the reference's special points."""
+    mp.mp.dps = 50
+    rng = np.random.default_rng(12)
+    d = {}
+    for name, f in SPH01.items():
+        z = np.concatenate([rng.uniform(-30.0, 30.0, 500), lu(rng, 1e-8, 600.0, 500) * rng.choice([-1.0, 1.0], 500)])
+        if name.startswith("spherical_bessel_k"):
+            z = np.abs(z)
+        if name in ("spherical_bessel_j_0", "spherical_bessel_j_1", "spherical_bessel_y_0", "spherical_bessel_y_1"):
+            g0 = {"j_0": lambda k: k * mp.pi, "j_1": lambda k: mp.besseljzero(1.5, k),
+                  "y_0": lambda k: (k - 0.5) * mp.pi, "y_1": lambda k: mp.besselyzero(1.5, k)}
+            zr = np.array([float(g0[name[-3:]](k)) for k in range(1, 11)])
+            z = np.concatenate([z, np.repeat(zr, 6) * (1 + rng.choice([-1.0, 1.0], 60) * lu(rng, 1e-10, 1e-4, 60))])
+        g, gg = rng.standard_normal(z.size), rng.standard_normal(z.size)
+        t = np.array([[float(mp.diff(f, mp.mpf(v), k)) if k else float(f(mp.mpf(v))) for k in range(3)] for v in z])
+        d[f"{name}_z"], d[f"{name}_g"], d[f"{name}_gg"], d[f"{name}_truth"] = z, g, gg, t
+        d[f"{name}_ref"] = ref(name, 0, z)[0]
+        d[f"{name}_ref_grad"] = ref(name, 1, g, z)[0]
+        d[f"{name}_ref_bb"] = np.stack(ref(name, 2, gg, g, z), axis=1)
+        sz = np.array([0.0, -0.0, 1e-13, -1e-13, -1.0, np.inf, -np.inf, np.nan])
+        d[f"{name}_special_z"] = sz
+        d[f"{name}_special_ref"] = ref(name, 0, sz)[0]
+        d[f"{name}_special_ref_grad"] = ref(name, 1, np.ones_like(sz), sz)[0]
+    mp.mp.dps = 40
+    np.savez_compressed(OUT / "spherical01.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family", "bessel_int"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family", "bessel_int", "spherical01"]
     for w in which:
         globals()[w]()
         print("wrote", w)

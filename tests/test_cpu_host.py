@@ -21,6 +21,22 @@ REFERENCE_SCHEMAS = [
     "regularized_gamma_p_backward_backward(Tensor grad_grad_a, Tensor grad_grad_x, Tensor grad, Tensor a, Tensor x) -> (Tensor, Tensor, Tensor)",
     "regularized_gamma_q(Tensor a, Tensor x) -> Tensor",
     "bessel_j_0(Tensor z) -> Tensor",
+    "spherical_bessel_j_0(Tensor z) -> Tensor",
+    "spherical_bessel_j_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
+    "spherical_bessel_j_1(Tensor z) -> Tensor",
+    "spherical_bessel_j_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
+    "spherical_bessel_y_0(Tensor z) -> Tensor",
+    "spherical_bessel_y_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
+    "spherical_bessel_y_1(Tensor z) -> Tensor",
+    "spherical_bessel_y_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
+    "spherical_bessel_i_0(Tensor z) -> Tensor",
+    "spherical_bessel_i_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
+    "spherical_bessel_i_1(Tensor z) -> Tensor",
+    "spherical_bessel_i_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
+    "spherical_bessel_k_0(Tensor z) -> Tensor",
+    "spherical_bessel_k_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
+    "spherical_bessel_k_1(Tensor z) -> Tensor",
+    "spherical_bessel_k_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
     "bessel_j_1(Tensor z) -> Tensor",
     "bessel_j_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
     "bessel_y_0(Tensor z) -> Tensor",

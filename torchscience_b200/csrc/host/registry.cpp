@@ -30,6 +30,17 @@ inline bool any_cuda(std::initializer_list<at::Tensor> ts) {
   return false;
 }
 
+// Tensors of a trace (torch.compile / export: fake or functional tensors)
+// carry no data, so the autograd code must not call the C ABI on them: their
+// kernels go through the dispatcher, which routes them to the Meta kernels.
+inline bool any_traced(std::initializer_list<at::Tensor> ts) {
+  for (const auto& t : ts)
+    if (t.defined() && (t.is_meta() || t.key_set().has(c10::DispatchKey::Python) ||
+                        t.key_set().has(c10::DispatchKey::Functionalize)))
+      return true;
+  return false;
+}
+
 // An autograd Function cannot return undefined tensors: gradients that were
 // not requested (and so not computed) come back as a zero expanded to the
 // input's shape, which allocates one element.
@@ -185,7 +196,7 @@ inline torch::autograd::variable_list defined_or_zero(std::vector<at::Tensor> r,
       ctx->saved_data["ra"] = ra;                                                                      \
       ctx->saved_data["rb"] = rb;                                                                      \
       at::AutoDispatchBelowAutograd guard;                                                             \
-      if (any_cuda({g, a, b})) {                                                                       \
+      if (any_cuda({g, a, b}) && !any_traced({g, a, b})) {                                             \
         /* Gradients come back already reduced to a's and b's shapes. */                               \
         return defined_or_zero(run_reduced_backward(BWD, #name "_backward", g, {a, b}, {ra, rb}), {a, b}); \
       }                                                                                                 \
@@ -308,7 +319,7 @@ inline torch::autograd::variable_list defined_or_zero(std::vector<at::Tensor> r,
       ctx->saved_data["ra"] = ra;                                                                               \
       ctx->saved_data["rb"] = rb;                                                                               \
       at::AutoDispatchBelowAutograd guard;                                                                      \
-      if ((ra || rb) && recorded && any_cuda({a, b})) {                                                         \
+      if ((ra || rb) && recorded && any_cuda({a, b}) && !any_traced({a, b})) {                                 \
         auto r = run_pointwise_masked(FWDGRAD, #name, {a, b}, 3, {true, ra, rb});                               \
         ctx->save_for_backward({a, b, r[1], r[2]});                                                             \
         ctx->saved_data["fused"] = true;                                                                        \
@@ -369,6 +380,14 @@ TSBH_UNARY_OP(modified_bessel_i_0, ModifiedBesselI0, z, tsb_modified_bessel_i_0,
 TSBH_UNARY_OP(modified_bessel_i_1, ModifiedBesselI1, z, tsb_modified_bessel_i_1, tsb_modified_bessel_i_1_backward, tsb_modified_bessel_i_1_backward_backward)
 TSBH_UNARY_OP(modified_bessel_k_0, ModifiedBesselK0, z, tsb_modified_bessel_k_0, tsb_modified_bessel_k_0_backward, tsb_modified_bessel_k_0_backward_backward)
 TSBH_UNARY_OP(modified_bessel_k_1, ModifiedBesselK1, z, tsb_modified_bessel_k_1, tsb_modified_bessel_k_1_backward, tsb_modified_bessel_k_1_backward_backward)
+TSBH_UNARY_OP(spherical_bessel_j_0, SphericalBesselJ0, z, tsb_spherical_bessel_j_0, tsb_spherical_bessel_j_0_backward, tsb_spherical_bessel_j_0_backward_backward)
+TSBH_UNARY_OP(spherical_bessel_j_1, SphericalBesselJ1, z, tsb_spherical_bessel_j_1, tsb_spherical_bessel_j_1_backward, tsb_spherical_bessel_j_1_backward_backward)
+TSBH_UNARY_OP(spherical_bessel_y_0, SphericalBesselY0, z, tsb_spherical_bessel_y_0, tsb_spherical_bessel_y_0_backward, tsb_spherical_bessel_y_0_backward_backward)
+TSBH_UNARY_OP(spherical_bessel_y_1, SphericalBesselY1, z, tsb_spherical_bessel_y_1, tsb_spherical_bessel_y_1_backward, tsb_spherical_bessel_y_1_backward_backward)
+TSBH_UNARY_OP(spherical_bessel_i_0, SphericalBesselI0, z, tsb_spherical_bessel_i_0, tsb_spherical_bessel_i_0_backward, tsb_spherical_bessel_i_0_backward_backward)
+TSBH_UNARY_OP(spherical_bessel_i_1, SphericalBesselI1, z, tsb_spherical_bessel_i_1, tsb_spherical_bessel_i_1_backward, tsb_spherical_bessel_i_1_backward_backward)
+TSBH_UNARY_OP(spherical_bessel_k_0, SphericalBesselK0, z, tsb_spherical_bessel_k_0, tsb_spherical_bessel_k_0_backward, tsb_spherical_bessel_k_0_backward_backward)
+TSBH_UNARY_OP(spherical_bessel_k_1, SphericalBesselK1, z, tsb_spherical_bessel_k_1, tsb_spherical_bessel_k_1_backward, tsb_spherical_bessel_k_1_backward_backward)
 TSBH_BINARY_OP(bessel_j, BesselJ, n, z, tsb_bessel_j, tsb_bessel_j_backward, tsb_bessel_j_backward_backward)
 TSBH_BINARY_OP(bessel_y, BesselY, n, z, tsb_bessel_y, tsb_bessel_y_backward, tsb_bessel_y_backward_backward)
 TSBH_BINARY_OP(modified_bessel_i, ModifiedBesselI, n, z, tsb_modified_bessel_i, tsb_modified_bessel_i_backward,
@@ -438,7 +457,7 @@ class Hypergeometric2F1Backward : public torch::autograd::Function<Hypergeometri
     ctx->save_for_backward({g, a, b, c, z});
     for (int i = 0; i < 4; ++i) ctx->saved_data["r" + std::to_string(i)] = static_cast<bool>(want[i]);
     at::AutoDispatchBelowAutograd guard;
-    if (any_cuda({g, a, b, c, z})) {
+    if (any_cuda({g, a, b, c, z}) && !any_traced({g, a, b, c, z})) {
       /* Gradients come back already reduced to the inputs' shapes. */
       return defined_or_zero(run_reduced_backward(tsb_hypergeometric_2_f_1_backward, "hypergeometric_2_f_1_backward",
                                                   g, {a, b, c, z}, want),

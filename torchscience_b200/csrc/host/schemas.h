@@ -65,6 +65,38 @@
   (m).def("modified_bessel_k_1(Tensor z) -> Tensor");                                                                  \
   (m).def("modified_bessel_k_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                     \
   (m).def("modified_bessel_k_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");     \
+  /* torchscience.cpp:922-924 */                                                                                       \
+  (m).def("spherical_bessel_j_0(Tensor z) -> Tensor");                                                                 \
+  (m).def("spherical_bessel_j_0_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
+  (m).def("spherical_bessel_j_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
+  /* torchscience.cpp:927-929 */                                                                                       \
+  (m).def("spherical_bessel_j_1(Tensor z) -> Tensor");                                                                 \
+  (m).def("spherical_bessel_j_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
+  (m).def("spherical_bessel_j_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
+  /* torchscience.cpp:937-939 */                                                                                       \
+  (m).def("spherical_bessel_y_0(Tensor z) -> Tensor");                                                                 \
+  (m).def("spherical_bessel_y_0_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
+  (m).def("spherical_bessel_y_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
+  /* torchscience.cpp:942-944 */                                                                                       \
+  (m).def("spherical_bessel_y_1(Tensor z) -> Tensor");                                                                 \
+  (m).def("spherical_bessel_y_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
+  (m).def("spherical_bessel_y_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
+  /* torchscience.cpp:952-954 */                                                                                       \
+  (m).def("spherical_bessel_i_0(Tensor z) -> Tensor");                                                                 \
+  (m).def("spherical_bessel_i_0_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
+  (m).def("spherical_bessel_i_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
+  /* torchscience.cpp:957-959 */                                                                                       \
+  (m).def("spherical_bessel_i_1(Tensor z) -> Tensor");                                                                 \
+  (m).def("spherical_bessel_i_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
+  (m).def("spherical_bessel_i_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
+  /* torchscience.cpp:967-969 */                                                                                       \
+  (m).def("spherical_bessel_k_0(Tensor z) -> Tensor");                                                                 \
+  (m).def("spherical_bessel_k_0_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
+  (m).def("spherical_bessel_k_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
+  /* torchscience.cpp:972-974 */                                                                                       \
+  (m).def("spherical_bessel_k_1(Tensor z) -> Tensor");                                                                 \
+  (m).def("spherical_bessel_k_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
+  (m).def("spherical_bessel_k_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
   /* torchscience.cpp:837-839 */                                                                                     \
   (m).def("hypergeometric_2_f_1(Tensor a, Tensor b, Tensor c, Tensor z) -> Tensor");                                 \
   (m).def(                                                                                                           \

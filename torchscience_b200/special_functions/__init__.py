@@ -209,6 +209,70 @@ def modified_bessel_k_1(z: Tensor) -> Tensor:
     return torch.ops.torchscience.modified_bessel_k_1(z)
 
 
+def spherical_bessel_j_0(z: Tensor) -> Tensor:
+    """Spherical Bessel function j_0(z) = sin(z)/z.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_j_0.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_j_0(z)
+
+
+def spherical_bessel_j_1(z: Tensor) -> Tensor:
+    """Spherical Bessel function j_1(z) = sin(z)/z² - cos(z)/z (series below |z| = 1).
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_j_1.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_j_1(z)
+
+
+def spherical_bessel_y_0(z: Tensor) -> Tensor:
+    """Spherical Bessel function y_0(z) = -cos(z)/z; -inf at 0.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_y_0.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_y_0(z)
+
+
+def spherical_bessel_y_1(z: Tensor) -> Tensor:
+    """Spherical Bessel function y_1(z) = -cos(z)/z² - sin(z)/z; -inf at 0.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_y_1.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_y_1(z)
+
+
+def spherical_bessel_i_0(z: Tensor) -> Tensor:
+    """Modified spherical Bessel function i_0(z) = sinh(z)/z.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_i_0.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_i_0(z)
+
+
+def spherical_bessel_i_1(z: Tensor) -> Tensor:
+    """Modified spherical Bessel function i_1(z) = cosh(z)/z - sinh(z)/z² (series below |z| = 1).
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_i_1.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_i_1(z)
+
+
+def spherical_bessel_k_0(z: Tensor) -> Tensor:
+    """Modified spherical Bessel function k_0(z) = (π/2) e^-z / z.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_k_0.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_k_0(z)
+
+
+def spherical_bessel_k_1(z: Tensor) -> Tensor:
+    """Modified spherical Bessel function k_1(z) = (π/2)(1 + z) e^-z / z²; +inf below |z| = 1e-12.
+
+    Same signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_k_1.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_k_1(z)
+
+
 __all__ = [
     "bessel_j",
     "bessel_j_0",
@@ -233,5 +297,13 @@ __all__ = [
     "polygamma",
     "regularized_gamma_p",
     "regularized_gamma_q",
+    "spherical_bessel_i_0",
+    "spherical_bessel_i_1",
+    "spherical_bessel_j_0",
+    "spherical_bessel_j_1",
+    "spherical_bessel_k_0",
+    "spherical_bessel_k_1",
+    "spherical_bessel_y_0",
+    "spherical_bessel_y_1",
     "trigamma",
 ]
