@@ -264,6 +264,26 @@ TSB_OP_SIGNATURE(tsb_spherical_bessel_k_1);
 TSB_OP_SIGNATURE(tsb_spherical_bessel_k_1_backward);
 TSB_OP_SIGNATURE(tsb_spherical_bessel_k_1_backward_backward);
 
+/* ---- Spherical Bessel functions of real order (n, z) ----------------------- */
+/* f_n(z) = sqrt(pi/(2|z|)) C_{n+1/2}(|z|), C = J, Y, I, K, with the reference's conventions for z < 0 and
+ * |z| < 1e-12; backward outputs {grad_n (central difference in n), grad_z}. */
+/* spherical_bessel_j(n, z): kernel/special_functions/spherical_bessel_j.h, schema torchscience.cpp:932-934. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_j_backward_backward);
+/* spherical_bessel_y(n, z): kernel/special_functions/spherical_bessel_y.h, schema torchscience.cpp:947-949. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_y_backward_backward);
+/* spherical_bessel_i(n, z): kernel/special_functions/spherical_bessel_i.h, schema torchscience.cpp:962-964. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_i_backward_backward);
+/* spherical_bessel_k(n, z): kernel/special_functions/spherical_bessel_k.h, schema torchscience.cpp:977-979. */
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k_backward);
+TSB_OP_SIGNATURE(tsb_spherical_bessel_k_backward_backward);
+
 /* ---- Fused forward for autograd (no counterpart in the reference) -------- */
 /* regularized_gamma_p / _q with their first derivatives in one evaluation: in = {a, x}, out =
  * {P (Q), d/da, d/dx} at the broadcast shape; a NULL d/da output is skipped.  The autograd forward of

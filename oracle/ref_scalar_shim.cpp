@@ -81,6 +81,18 @@
 #include "kernel/special_functions/spherical_bessel_k_1.h"
 #include "kernel/special_functions/spherical_bessel_k_1_backward.h"
 #include "kernel/special_functions/spherical_bessel_k_1_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_j.h"
+#include "kernel/special_functions/spherical_bessel_j_backward.h"
+#include "kernel/special_functions/spherical_bessel_j_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_y.h"
+#include "kernel/special_functions/spherical_bessel_y_backward.h"
+#include "kernel/special_functions/spherical_bessel_y_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_i.h"
+#include "kernel/special_functions/spherical_bessel_i_backward.h"
+#include "kernel/special_functions/spherical_bessel_i_backward_backward.h"
+#include "kernel/special_functions/spherical_bessel_k.h"
+#include "kernel/special_functions/spherical_bessel_k_backward.h"
+#include "kernel/special_functions/spherical_bessel_k_backward_backward.h"
 #include "kernel/special_functions/bessel_j.h"
 #include "kernel/special_functions/bessel_j_0.h"
 #include "kernel/special_functions/bessel_j_0_backward.h"
@@ -224,6 +236,10 @@ static int eval_typed(const char* name, int pass, const void* const* in, void* c
   BINARY(bessel_y)
   BINARY(modified_bessel_i)
   BINARY(modified_bessel_k)
+  BINARY(spherical_bessel_j)
+  BINARY(spherical_bessel_y)
+  BINARY(spherical_bessel_i)
+  BINARY(spherical_bessel_k)
   BINARY(log_beta)
   BINARY(beta)
   BINARY(polygamma)

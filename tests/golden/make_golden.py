@@ -546,8 +546,61 @@ def spherical01():
     np.savez_compressed(OUT / "spherical01.npz", **d)
 
 
+def _sph_truth(kind, n, z):
+    """The reference's convention of the spherical Bessel function of real order
+    at 40 digits: sqrt(pi/(2|z|)) C_{n+1/2}(|z|) times, for z < 0, the factor
+    (-1)^n or cos(pi n) (y: n + 1)."""
+    fn = {"j": mp.besselj, "y": mp.bessely, "i": mp.besseli, "k": mp.besselk}[kind]
+    az = abs(z)
+    v = mp.sqrt(mp.pi / (2 * az)) * fn(n + mp.mpf(1) / 2, az)
+    if z < 0:
+        m = n + 1 if kind == "y" else n
+        v *= mp.cos(mp.pi * m)
+    return mp.re(v)
+
+
+def spherical():
+    """Spherical Bessel functions of real order n: n in {0..10} and U(-2.5, 10),
+    z in U(0.05, 40) and LogU(1e-6, 300), negative z for j, y, i; mpmath values,
+    d/dz and d/dn (40 digits), second derivatives on a subsample; the
+    reference's forward and backward outputs and its special points."""
+    rng = np.random.default_rng(13)
+    d = {}
+    for kind in "jyik":
+        name = f"spherical_bessel_{kind}"
+        m = 400
+        n = np.where(rng.random(m) < 0.5, rng.integers(0, 11, m).astype(float), rng.uniform(-2.5, 10.0, m))
+        z = np.where(rng.random(m) < 0.5, rng.uniform(0.05, 40.0, m), lu(rng, 1e-6, 300.0, m))
+        if kind != "k":
+            z = z * np.where(rng.random(m) < 0.2, -1.0, 1.0)
+        g = rng.standard_normal(m)
+        t = []
+        for a, b in zip(n, z):
+            A, Bz = mp.mpf(a), mp.mpf(b)
+            t.append([float(_sph_truth(kind, A, Bz)), float(mp.diff(lambda u: _sph_truth(kind, A, u), Bz)),
+                      float(mp.diff(lambda u: _sph_truth(kind, u, Bz), A))])
+        d[f"{name}_n"], d[f"{name}_z"], d[f"{name}_g"] = n, z, g
+        d[f"{name}_truth"] = np.array(t)
+        idx = np.arange(0, m, 4)
+        t2 = []
+        for i in idx:
+            A, Bz = mp.mpf(n[i]), mp.mpf(z[i])
+            t2.append([float(mp.diff(lambda u: _sph_truth(kind, A, u), Bz, 2)),
+                       float(mp.diff(lambda u, w: _sph_truth(kind, u, w), (A, Bz), (1, 1))),
+                       float(mp.diff(lambda u: _sph_truth(kind, u, Bz), A, 2))])
+        d[f"{name}_idx2"], d[f"{name}_truth2"] = idx, np.array(t2)
+        d[f"{name}_ref"] = ref(name, 0, n, z)[0]
+        d[f"{name}_ref_grad"] = np.stack(ref(name, 1, g, n, z), axis=1)
+        sn = np.array([0.0, 1.0, 2.0, -0.5, 0.0, 1.0, 3.0, np.nan, 1.0])
+        sz = np.array([0.0, 0.0, 1e-13, 0.0, -1e-13, -2.0, -2.0, 1.0, np.nan])
+        d[f"{name}_special_n"], d[f"{name}_special_z"] = sn, sz
+        d[f"{name}_special_ref"] = ref(name, 0, sn, sz)[0]
+        d[f"{name}_special_ref_grad"] = np.stack(ref(name, 1, np.ones_like(sn), sn, sz), axis=1)
+    np.savez_compressed(OUT / "spherical.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family", "bessel_int", "spherical01"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family", "bessel_int", "spherical01", "spherical"]
     for w in which:
         globals()[w]()
         print("wrote", w)

@@ -21,6 +21,14 @@ REFERENCE_SCHEMAS = [
     "regularized_gamma_p_backward_backward(Tensor grad_grad_a, Tensor grad_grad_x, Tensor grad, Tensor a, Tensor x) -> (Tensor, Tensor, Tensor)",
     "regularized_gamma_q(Tensor a, Tensor x) -> Tensor",
     "bessel_j_0(Tensor z) -> Tensor",
+    "spherical_bessel_j(Tensor n, Tensor z) -> Tensor",
+    "spherical_bessel_j_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor, Tensor)",
+    "spherical_bessel_y(Tensor n, Tensor z) -> Tensor",
+    "spherical_bessel_y_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor, Tensor)",
+    "spherical_bessel_i(Tensor n, Tensor z) -> Tensor",
+    "spherical_bessel_i_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor, Tensor)",
+    "spherical_bessel_k(Tensor n, Tensor z) -> Tensor",
+    "spherical_bessel_k_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor, Tensor)",
     "spherical_bessel_j_0(Tensor z) -> Tensor",
     "spherical_bessel_j_0_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)",
     "spherical_bessel_j_1(Tensor z) -> Tensor",

@@ -388,6 +388,10 @@ TSBH_UNARY_OP(spherical_bessel_i_0, SphericalBesselI0, z, tsb_spherical_bessel_i
 TSBH_UNARY_OP(spherical_bessel_i_1, SphericalBesselI1, z, tsb_spherical_bessel_i_1, tsb_spherical_bessel_i_1_backward, tsb_spherical_bessel_i_1_backward_backward)
 TSBH_UNARY_OP(spherical_bessel_k_0, SphericalBesselK0, z, tsb_spherical_bessel_k_0, tsb_spherical_bessel_k_0_backward, tsb_spherical_bessel_k_0_backward_backward)
 TSBH_UNARY_OP(spherical_bessel_k_1, SphericalBesselK1, z, tsb_spherical_bessel_k_1, tsb_spherical_bessel_k_1_backward, tsb_spherical_bessel_k_1_backward_backward)
+TSBH_BINARY_OP(spherical_bessel_j, SphericalBesselJ, n, z, tsb_spherical_bessel_j, tsb_spherical_bessel_j_backward, tsb_spherical_bessel_j_backward_backward)
+TSBH_BINARY_OP(spherical_bessel_y, SphericalBesselY, n, z, tsb_spherical_bessel_y, tsb_spherical_bessel_y_backward, tsb_spherical_bessel_y_backward_backward)
+TSBH_BINARY_OP(spherical_bessel_i, SphericalBesselI, n, z, tsb_spherical_bessel_i, tsb_spherical_bessel_i_backward, tsb_spherical_bessel_i_backward_backward)
+TSBH_BINARY_OP(spherical_bessel_k, SphericalBesselK, n, z, tsb_spherical_bessel_k, tsb_spherical_bessel_k_backward, tsb_spherical_bessel_k_backward_backward)
 TSBH_BINARY_OP(bessel_j, BesselJ, n, z, tsb_bessel_j, tsb_bessel_j_backward, tsb_bessel_j_backward_backward)
 TSBH_BINARY_OP(bessel_y, BesselY, n, z, tsb_bessel_y, tsb_bessel_y_backward, tsb_bessel_y_backward_backward)
 TSBH_BINARY_OP(modified_bessel_i, ModifiedBesselI, n, z, tsb_modified_bessel_i, tsb_modified_bessel_i_backward,

@@ -97,6 +97,30 @@
   (m).def("spherical_bessel_k_1(Tensor z) -> Tensor");                                                                 \
   (m).def("spherical_bessel_k_1_backward(Tensor grad_output, Tensor z) -> Tensor");                                    \
   (m).def("spherical_bessel_k_1_backward_backward(Tensor gg_z, Tensor grad_output, Tensor z) -> (Tensor, Tensor)");    \
+  /* torchscience.cpp:932-934 */                                                                                       \
+  (m).def("spherical_bessel_j(Tensor n, Tensor z) -> Tensor");                                                         \
+  (m).def("spherical_bessel_j_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                  \
+  (m).def(                                                                                                             \
+      "spherical_bessel_j_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> "     \
+      "(Tensor, Tensor, Tensor)");                                                                                     \
+  /* torchscience.cpp:947-949 */                                                                                       \
+  (m).def("spherical_bessel_y(Tensor n, Tensor z) -> Tensor");                                                         \
+  (m).def("spherical_bessel_y_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                  \
+  (m).def(                                                                                                             \
+      "spherical_bessel_y_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> "     \
+      "(Tensor, Tensor, Tensor)");                                                                                     \
+  /* torchscience.cpp:962-964 */                                                                                       \
+  (m).def("spherical_bessel_i(Tensor n, Tensor z) -> Tensor");                                                         \
+  (m).def("spherical_bessel_i_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                  \
+  (m).def(                                                                                                             \
+      "spherical_bessel_i_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> "     \
+      "(Tensor, Tensor, Tensor)");                                                                                     \
+  /* torchscience.cpp:977-979 */                                                                                       \
+  (m).def("spherical_bessel_k(Tensor n, Tensor z) -> Tensor");                                                         \
+  (m).def("spherical_bessel_k_backward(Tensor grad_output, Tensor n, Tensor z) -> (Tensor, Tensor)");                  \
+  (m).def(                                                                                                             \
+      "spherical_bessel_k_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> "     \
+      "(Tensor, Tensor, Tensor)");                                                                                     \
   /* torchscience.cpp:837-839 */                                                                                     \
   (m).def("hypergeometric_2_f_1(Tensor a, Tensor b, Tensor c, Tensor z) -> Tensor");                                 \
   (m).def(                                                                                                           \

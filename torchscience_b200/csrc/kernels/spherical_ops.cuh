@@ -155,3 +155,153 @@ TSB_SPH01_ALIASES(SphK1, kSphK, 1)
 #undef TSB_SPH01_ALIASES
 
 }  // namespace tsb
+
+// ---- spherical Bessel functions of real order n: spherical_bessel_{j,y,i,k}(n, z)
+// f_n(z) = sqrt(π/(2|z|)) C_{n+1/2}(|z|) with C = J, Y, I, K (DLMF 10.47.3, 10.47.7,
+// 10.47.8 with the reference's normalisation of k), evaluated by the real-order
+// Bessel evaluators, with the reference's conventions (spherical_bessel_j.h,
+// _y.h, _i.h, _k.h; the `spherical_bessel_*(T n, T z)` functions):
+//   - n within 1e-12 of an integer counts as that integer; |z| < 1e-12 counts
+//     as 0: j, i = 1 at n = 0, 0 for n > 0, inf for n < 0; y = -inf; k = +inf;
+//     ∂/∂z there: j, i 0 (1/3 at n = 1, NaN for n < 0); y, k -inf;
+//   - z < 0: k is NaN; j, i take the factor (-1)^n for integer n and cos(πn)
+//     otherwise, y the factor (-1)^(n+1) or cos(π(n+1));
+//   - ∂/∂n by central differences of this function (step ε^(1/3) max(1, |n|),
+//     ε^(1/4) for the second derivative), as the reference differentiates in n
+//     numerically; ∂/∂z from the evaluator (below |z| = 1 from the order
+//     recurrence, since C' - C/(2z) cancels there), ∂²/∂z² from the spherical
+//     Bessel equation.
+
+#include "bessel_ops.cuh"
+
+namespace tsb {
+
+constexpr double kSphEps = 1e-12;
+
+template <int KIND>
+__device__ inline double sph_phase(double n) {  // factor for z < 0 (j, y, i)
+  const double nr = rint(n);
+  const double m = KIND == kSphY ? 1.0 : 0.0;
+  if (fabs(n - nr) < kSphEps) return fmod(fabs(nr + m), 2.0) == 1.0 ? -1.0 : 1.0;
+  double s, c;
+  sincospi(n + m, &s, &c);
+  return c;
+}
+
+// f_n(z) and ∂f/∂z (and, when D2, ∂²f/∂z²) with the conventions above.
+template <int KIND, bool D2>
+__device__ inline SphVals sph_eval(double n, double z) {
+  const double nan = CUDART_NAN, inf = CUDART_INF;
+  if (isnan(n) || isnan(z)) return {nan, nan, nan};
+  if (fabs(z) < kSphEps) {
+    double v;
+    if (KIND == kSphY) v = -inf;
+    else if (KIND == kSphK) v = inf;
+    else v = fabs(n) < kSphEps ? 1.0 : (n > 0.0 ? 0.0 : inf);
+    double d = -inf;  // y, k: the reference's value at the pole
+    if (KIND == kSphJ || KIND == kSphI) d = fabs(n) < kSphEps ? 0.0 : (fabs(n - 1.0) < kSphEps ? 1.0 / 3.0 : (n > 0.0 ? 0.0 : nan));
+    return {v, d, nan};
+  }
+  if (KIND == kSphK && z < 0.0) return {nan, nan, nan};
+  const double nr = rint(n);
+  const double nn = (n >= 0.0 && fabs(n - nr) < kSphEps) ? nr : n;  // the order used
+  const double az = fabs(z), nu = nn + 0.5;
+  BV<double> b;
+  if (KIND == kSphJ) b = bessel_eval<double, kBJ>(nu, az);
+  else if (KIND == kSphY) b = bessel_eval<double, kBY>(nu, az);
+  else if (KIND == kSphI) b = bessel_eval<double, kBI>(nu, az);
+  else b = bessel_eval<double, kBK>(nu, az);
+  if (isinf(az)) return {b.v == b.v ? (KIND == kSphI ? b.v : 0.0) : nan, 0.0, 0.0};
+  const double pre = sqrt(1.5707963267948966 / az);
+  double v = pre * b.v, d;
+  if (az < 1.0) {
+    // C' - C/(2z) cancels as z -> 0: the order recurrence instead,
+    // d/dz [pre C_ν] = pre ((n/z) C_ν - C_{ν+1}) (J, Y, K), pre ((n/z) I_ν + I_{ν+1}) (I)
+    double c1;
+    if (KIND == kSphJ) c1 = bessel_eval<double, kBJ>(nu + 1.0, az).v;
+    else if (KIND == kSphY) c1 = bessel_eval<double, kBY>(nu + 1.0, az).v;
+    else if (KIND == kSphI) c1 = bessel_eval<double, kBI>(nu + 1.0, az).v;
+    else c1 = bessel_eval<double, kBK>(nu + 1.0, az).v;
+    d = pre * fma(nn / az, b.v, KIND == kSphI ? c1 : -c1);
+  } else {
+    d = pre * (b.d - 0.5 * b.v / az);
+  }
+  double d2 = 0.0;
+  if (D2) {
+    const double r = 1.0 / az, q = nn * (nn + 1.0) * r * r;
+    d2 = (KIND == kSphJ || KIND == kSphY) ? -2.0 * d * r - (1.0 - q) * v : -2.0 * d * r + (1.0 + q) * v;
+  }
+  if (z < 0.0) {  // f(z) = φ g(|z|): f' = -φ g', f'' = φ g''
+    const double ph = sph_phase<KIND>(n);
+    v *= ph;
+    d *= -ph;
+    d2 *= ph;
+  }
+  return {v, d, d2};
+}
+
+struct SphNuDerivs {
+  double dn, dnz, dnn;  // ∂f/∂n, ∂²f/∂n∂z, ∂²f/∂n²
+};
+template <int KIND, bool SECOND>
+__device__ inline SphNuDerivs sph_nu_derivs(double n, double z, double f0) {
+  SphNuDerivs o{0.0, 0.0, 0.0};
+  const double h = 6.0554544523933395e-06 * fmax(1.0, fabs(n));
+  const SphVals p = sph_eval<KIND, false>(n + h, z), m = sph_eval<KIND, false>(n - h, z);
+  o.dn = (p.v - m.v) / (2.0 * h);
+  o.dnz = (p.d - m.d) / (2.0 * h);
+  if (SECOND) {
+    const double h2 = 1.2207031250e-04 * fmax(1.0, fabs(n));
+    const double vp = sph_eval<KIND, false>(n + h2, z).v, vm = sph_eval<KIND, false>(n - h2, z).v;
+    o.dnn = (vp - 2.0 * f0 + vm) / (h2 * h2);
+  }
+  return o;
+}
+
+template <int KIND, typename T_>
+struct SphFwd {  // in = {n, z}
+  using T = T_;
+  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    out[0] = (T)sph_eval<KIND, false>((double)in[0], (double)in[1]).v;
+  }
+};
+template <int KIND, typename T_>
+struct SphBwd {  // in = {grad, n, z}, out = {grad_n, grad_z}
+  using T = T_;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t mask) {
+    const double g = in[0], n = in[1], z = in[2];
+    const SphVals f = sph_eval<KIND, false>(n, z);
+    out[0] = (mask & 1u) ? (T)(g * sph_nu_derivs<KIND, false>(n, z, f.v).dn) : T(0);
+    out[1] = (T)(g * f.d);
+  }
+};
+template <int KIND, typename T_>
+struct SphBwdBwd {  // in = {gg_n, gg_z, grad, n, z}, out = {grad_grad_output, grad_n, grad_z}
+  using T = T_;
+  static constexpr int NIN = 5, NOUT = 3, R = 1;
+  static constexpr bool REDUCE = true;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const double ggn = in[0], ggz = in[1], g = in[2], n = in[3], z = in[4];
+    const SphVals f = sph_eval<KIND, true>(n, z);
+    const SphNuDerivs dn = sph_nu_derivs<KIND, true>(n, z, f.v);
+    out[0] = (T)(ggn * dn.dn + ggz * f.d);
+    out[1] = (T)(g * (ggn * dn.dnn + ggz * dn.dnz));
+    out[2] = (T)(g * (ggn * dn.dnz + ggz * f.d2));
+  }
+};
+
+#define TSB_SPH_ALIASES(Name, KIND)                                   \
+  template <typename T> using Name##Fwd = SphFwd<KIND, T>;           \
+  template <typename T> using Name##Bwd = SphBwd<KIND, T>;           \
+  template <typename T> using Name##BwdBwd = SphBwdBwd<KIND, T>;
+TSB_SPH_ALIASES(SphJ, kSphJ)
+TSB_SPH_ALIASES(SphY, kSphY)
+TSB_SPH_ALIASES(SphI, kSphI)
+TSB_SPH_ALIASES(SphK, kSphK)
+#undef TSB_SPH_ALIASES
+
+}  // namespace tsb

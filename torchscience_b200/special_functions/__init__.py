@@ -273,6 +273,42 @@ def spherical_bessel_k_1(z: Tensor) -> Tensor:
     return torch.ops.torchscience.spherical_bessel_k_1(z)
 
 
+def spherical_bessel_j(n: Tensor, z: Tensor) -> Tensor:
+    """Spherical Bessel function of the first kind j_n(z) = sqrt(π/(2z)) J_{n+1/2}(z) of real order n.
+
+    For z < 0 the reference's real-valued conventions apply ((-1)^n or cos(πn) factors).  Same
+    signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_j.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_j(n, z)
+
+
+def spherical_bessel_y(n: Tensor, z: Tensor) -> Tensor:
+    """Spherical Bessel function of the second kind y_n(z) = sqrt(π/(2z)) Y_{n+1/2}(z) of real order n.
+
+    For z < 0 the reference's real-valued conventions apply ((-1)^n or cos(πn) factors).  Same
+    signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_y.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_y(n, z)
+
+
+def spherical_bessel_i(n: Tensor, z: Tensor) -> Tensor:
+    """Modified spherical Bessel function i_n(z) = sqrt(π/(2z)) I_{n+1/2}(z) of real order n.
+
+    For z < 0 the reference's real-valued conventions apply ((-1)^n or cos(πn) factors).  Same
+    signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_i.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_i(n, z)
+
+
+def spherical_bessel_k(n: Tensor, z: Tensor) -> Tensor:
+    """Modified spherical Bessel function k_n(z) = sqrt(π/(2z)) K_{n+1/2}(z) of real order n; NaN for z < 0.
+
+    For z < 0 the reference's real-valued conventions apply ((-1)^n or cos(πn) factors).  Same
+    signature and semantics as the reference wrapper (src/torchscience/special_functions/_spherical_bessel_k.py).
+    """
+    return torch.ops.torchscience.spherical_bessel_k(n, z)
+
+
 __all__ = [
     "bessel_j",
     "bessel_j_0",
@@ -297,12 +333,16 @@ __all__ = [
     "polygamma",
     "regularized_gamma_p",
     "regularized_gamma_q",
+    "spherical_bessel_i",
     "spherical_bessel_i_0",
     "spherical_bessel_i_1",
+    "spherical_bessel_j",
     "spherical_bessel_j_0",
     "spherical_bessel_j_1",
+    "spherical_bessel_k",
     "spherical_bessel_k_0",
     "spherical_bessel_k_1",
+    "spherical_bessel_y",
     "spherical_bessel_y_0",
     "spherical_bessel_y_1",
     "trigamma",
