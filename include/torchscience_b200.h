@@ -284,6 +284,14 @@ TSB_OP_SIGNATURE(tsb_spherical_bessel_k);
 TSB_OP_SIGNATURE(tsb_spherical_bessel_k_backward);
 TSB_OP_SIGNATURE(tsb_spherical_bessel_k_backward_backward);
 
+/* ---- Regularized incomplete beta I_x(a, b) --------------------------------- */
+/* incomplete_beta(x, a, b): kernel/special_functions/incomplete_beta.h:27-63, schema torchscience.cpp:833-835;
+ * backward incomplete_beta_backward.h:212-276 (outputs {grad_x, grad_a, grad_b}); double backward
+ * incomplete_beta_backward_backward.h:110-237 (outputs {grad_grad_output, grad_x, grad_a, grad_b}). */
+TSB_OP_SIGNATURE(tsb_incomplete_beta);
+TSB_OP_SIGNATURE(tsb_incomplete_beta_backward);
+TSB_OP_SIGNATURE(tsb_incomplete_beta_backward_backward);
+
 /* ---- Fused forward for autograd (no counterpart in the reference) -------- */
 /* regularized_gamma_p / _q with their first derivatives in one evaluation: in = {a, x}, out =
  * {P (Q), d/da, d/dx} at the broadcast shape; a NULL d/da output is skipped.  The autograd forward of

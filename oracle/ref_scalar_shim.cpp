@@ -30,6 +30,9 @@
 #include "kernel/special_functions/beta.h"
 #include "kernel/special_functions/beta_backward.h"
 #include "kernel/special_functions/beta_backward_backward.h"
+#include "kernel/special_functions/incomplete_beta.h"
+#include "kernel/special_functions/incomplete_beta_backward.h"
+#include "kernel/special_functions/incomplete_beta_backward_backward.h"
 #include "kernel/special_functions/log_beta.h"
 #include "kernel/special_functions/log_beta_backward.h"
 #include "kernel/special_functions/log_beta_backward_backward.h"
@@ -271,6 +274,12 @@ static int eval_typed(const char* name, int pass, const void* const* in, void* c
   if (std::strcmp(name, "chi2_probability_density") == 0) {
     if (pass == 0) LOOP(pr::chi2_probability_density(ARG(0), ARG(1)));
     if (pass == 1) LOOP(pr::chi2_probability_density_backward(ARG(0), ARG(1), ARG(2)));
+    return -1;
+  }
+  if (std::strcmp(name, "incomplete_beta") == 0) {
+    if (pass == 0) LOOP(sf::incomplete_beta(ARG(0), ARG(1), ARG(2)));
+    if (pass == 1) LOOP(sf::incomplete_beta_backward(ARG(0), ARG(1), ARG(2), ARG(3)));
+    if (pass == 2) LOOP(sf::incomplete_beta_backward_backward(ARG(0), ARG(1), ARG(2), ARG(3), ARG(4), ARG(5), ARG(6)));
     return -1;
   }
   if (std::strcmp(name, "hypergeometric_2_f_1") == 0) {

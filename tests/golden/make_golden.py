@@ -599,8 +599,85 @@ def spherical():
     np.savez_compressed(OUT / "spherical.npz", **d)
 
 
+def _ibeta_truth(x, a, b):
+    """I_x(a, b) and its first derivatives at 40 digits.  Where I > 1/2 the
+    complement 1 - I_x(a, b) = I_(1-x)(b, a) is evaluated instead (its
+    value and parameter derivatives keep their relative accuracy when they
+    are tiny), and the a/b derivatives are its negatives."""
+    X, A, B = mp.mpf(x), mp.mpf(a), mp.mpf(b)
+    lo = mp.betainc(A, B, 0, X, regularized=True)
+    comp = lo > 0.5
+    if comp:
+        f = lambda u, v: mp.betainc(v, u, 0, 1 - X, regularized=True)  # noqa: E731
+        hi = f(A, B)
+        val = 1 - hi
+        da, db = -mp.diff(lambda u: f(u, B), A), -mp.diff(lambda v: f(A, v), B)
+    else:
+        f = lambda u, v: mp.betainc(u, v, 0, X, regularized=True)  # noqa: E731
+        val = lo
+        da, db = mp.diff(lambda u: f(u, B), A), mp.diff(lambda v: f(A, v), B)
+    pdf = mp.exp((A - 1) * mp.log(X) + (B - 1) * mp.log1p(-X)) / mp.beta(A, B)
+    return val, pdf, da, db, f, comp
+
+
+def incomplete_beta():
+    """incomplete_beta: seeded x in (0, 1), a and b log-uniform over
+    [0.05, 300] (a block drawn near the swap line x = (a+1)/(a+b+2), a block
+    with a or b near 1, a block of a, b in [300, 3000]); mpmath values (40
+    digits) of I, ∂x, ∂a, ∂b and, on every tenth point, the six second
+    derivatives; the reference's outputs; the reference's special points."""
+    rng = np.random.default_rng(14)
+    n = 600
+    a = lu(rng, 0.05, 300.0, n)
+    b = lu(rng, 0.05, 300.0, n)
+    x = rng.uniform(0.0, 1.0, n)
+    x[:100] = np.clip((a[:100] + 1) / (a[:100] + b[:100] + 2) * rng.uniform(0.9, 1.1, 100), 1e-6, 1 - 1e-6)
+    a[100:130] = 1.0 + rng.uniform(-1e-3, 1e-3, 30)
+    b[130:160] = 1.0 + rng.uniform(-1e-3, 1e-3, 30)
+    a[160:200] = lu(rng, 300.0, 3000.0, 40)
+    b[160:200] = lu(rng, 300.0, 3000.0, 40)
+    x[160:200] = np.clip(a[160:200] / (a[160:200] + b[160:200]) + rng.normal(0, 0.02, 40), 1e-3, 1 - 1e-3)
+    x[200:240] = lu(rng, 1e-8, 1e-2, 40)
+    x[240:280] = 1 - lu(rng, 1e-8, 1e-2, 40)
+    d = {"x": x, "a": a, "b": b, "g": rng.standard_normal(n)}
+    cols = {k: [] for k in ("v", "dx", "da", "db")}
+    idx2 = np.arange(0, n, 10)
+    sec = {k: [] for k in ("hxx", "hxa", "hxb", "haa", "hab", "hbb")}
+    for i in range(n):
+        val, pdf, da, db, f, comp = _ibeta_truth(x[i], a[i], b[i])
+        for k, v in zip(("v", "dx", "da", "db"), (val, pdf, da, db)):
+            cols[k].append(float(v))
+        if i in set(idx2.tolist()):
+            X, A, B = mp.mpf(x[i]), mp.mpf(a[i]), mp.mpf(b[i])
+            sgn = -1 if comp else 1
+            sec["hxx"].append(float(pdf * ((A - 1) / X - (B - 1) / (1 - X))))
+            sec["hxa"].append(float(pdf * (mp.log(X) - mp.digamma(A) + mp.digamma(A + B))))
+            sec["hxb"].append(float(pdf * (mp.log1p(-X) - mp.digamma(B) + mp.digamma(A + B))))
+            sec["haa"].append(float(sgn * mp.diff(lambda u, v: f(u, v), (A, B), (2, 0))))
+            sec["hab"].append(float(sgn * mp.diff(lambda u, v: f(u, v), (A, B), (1, 1))))
+            sec["hbb"].append(float(sgn * mp.diff(lambda u, v: f(u, v), (A, B), (0, 2))))
+    for k, v in cols.items():
+        d[f"truth_{k}"] = np.array(v)
+    d["idx2"] = idx2
+    for k, v in sec.items():
+        d[f"truth_{k}"] = np.array(v)
+    gg = rng.standard_normal((3, n))
+    d["gg"] = gg
+    d["ref"] = ref("incomplete_beta", 0, x, a, b)[0]
+    d["ref_grad"] = np.stack(ref("incomplete_beta", 1, d["g"], x, a, b), axis=1)
+    i2 = idx2
+    d["ref_bb"] = np.stack(ref("incomplete_beta", 2, gg[0][i2], gg[1][i2], gg[2][i2], d["g"][i2], x[i2], a[i2], b[i2]), axis=1)
+    sx = np.array([0.0, -0.5, 1.0, 1.5, 0.3, 0.3, 0.3, 0.3, 0.3, 0.4, 0.7, np.nan, 0.5, 0.5, 1e-300])
+    sa = np.array([2.0, 2.0, 2.0, 2.0, 0.0, -1.0, 1.0, 1.0, 2.5, 2.5, 1.0, 2.0, np.nan, 3.0, 2.0])
+    sb = np.array([3.0, 3.0, 3.0, 3.0, 2.0, 2.0, 1.0, 2.5, 1.0, 0.0, 3.0, 3.0, 2.0, np.nan, 3.0])
+    d["special_x"], d["special_a"], d["special_b"] = sx, sa, sb
+    d["special_ref"] = ref("incomplete_beta", 0, sx, sa, sb)[0]
+    d["special_ref_grad"] = np.stack(ref("incomplete_beta", 1, np.ones_like(sx), sx, sa, sb), axis=1)
+    np.savez_compressed(OUT / "incomplete_beta.npz", **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family", "bessel_int", "spherical01", "spherical"]
+    which = sys.argv[1:] or ["gamma_family", "igamma", "elliptic", "bessel", "bessel01", "hyp2f1", "probability", "probability_density", "beta_family", "bessel_int", "spherical01", "spherical", "incomplete_beta"]
     for w in which:
         globals()[w]()
         print("wrote", w)

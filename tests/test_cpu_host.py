@@ -70,6 +70,9 @@ REFERENCE_SCHEMAS = [
     "bessel_y(Tensor n, Tensor z) -> Tensor",
     "modified_bessel_i(Tensor n, Tensor z) -> Tensor",
     "modified_bessel_k(Tensor n, Tensor z) -> Tensor",
+    "incomplete_beta(Tensor x, Tensor a, Tensor b) -> Tensor",
+    "incomplete_beta_backward(Tensor grad_output, Tensor x, Tensor a, Tensor b) -> (Tensor, Tensor, Tensor)",
+    "incomplete_beta_backward_backward(Tensor gg_x, Tensor gg_a, Tensor gg_b, Tensor grad_output, Tensor x, Tensor a, Tensor b) -> (Tensor, Tensor, Tensor, Tensor)",
     "hypergeometric_2_f_1(Tensor a, Tensor b, Tensor c, Tensor z) -> Tensor",
     "hypergeometric_2_f_1_backward(Tensor grad_output, Tensor a, Tensor b, Tensor c, Tensor z) -> (Tensor, Tensor, Tensor, Tensor)",
     "complete_legendre_elliptic_integral_k(Tensor m) -> Tensor",

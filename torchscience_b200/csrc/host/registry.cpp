@@ -556,6 +556,146 @@ TORCH_LIBRARY_IMPL(torchscience, CPU, m) {
 TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_autograd); }
 TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl("hypergeometric_2_f_1", tsbh::ops::hyp2f1_autocast); }
 
+// ------------------------------------------------------------- I_x(a, b)
+// The one ternary special function (autograd structure as the binary ops
+// above, with three inputs).
+namespace tsbh::ops {
+using T3i = std::tuple<at::Tensor, at::Tensor, at::Tensor>;
+using T4i = std::tuple<at::Tensor, at::Tensor, at::Tensor, at::Tensor>;
+
+at::Tensor ibeta_cuda(const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+  return run_pointwise(tsb_incomplete_beta, "incomplete_beta", {x, a, b}, 1)[0];
+}
+T3i ibeta_backward_cuda(const at::Tensor& g, const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+  auto r = run_pointwise(tsb_incomplete_beta_backward, "incomplete_beta_backward", {g, x, a, b}, 3);
+  return {r[0], r[1], r[2]};
+}
+T4i ibeta_backward_backward_cuda(const at::Tensor& ggx, const at::Tensor& gga, const at::Tensor& ggb,
+                                 const at::Tensor& g, const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+  auto r = run_pointwise(tsb_incomplete_beta_backward_backward, "incomplete_beta_backward_backward",
+                         {ggx, gga, ggb, g, x, a, b}, 4);
+  return {r[0], r[1], r[2], r[3]};
+}
+at::Tensor ibeta_meta(const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+  return meta_pointwise("incomplete_beta", {x, a, b}, 1)[0];
+}
+T3i ibeta_backward_meta(const at::Tensor& g, const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+  auto r = meta_pointwise("incomplete_beta_backward", {g, x, a, b}, 3);
+  return {r[0], r[1], r[2]};
+}
+T4i ibeta_backward_backward_meta(const at::Tensor& ggx, const at::Tensor& gga, const at::Tensor& ggb,
+                                 const at::Tensor& g, const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+  auto r = meta_pointwise("incomplete_beta_backward_backward", {ggx, gga, ggb, g, x, a, b}, 4);
+  return {r[0], r[1], r[2], r[3]};
+}
+at::Tensor ibeta_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&) {
+  cpu_not_supported("incomplete_beta");
+}
+T3i ibeta_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&) {
+  cpu_not_supported("incomplete_beta_backward");
+}
+T4i ibeta_backward_backward_cpu(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                const at::Tensor&, const at::Tensor&, const at::Tensor&) {
+  cpu_not_supported("incomplete_beta_backward_backward");
+}
+
+class IncompleteBetaBackward : public torch::autograd::Function<IncompleteBetaBackward> {
+ public:
+  static variable_list forward(AutogradContext* ctx, const at::Tensor& g, const at::Tensor& x, const at::Tensor& a,
+                               const at::Tensor& b, std::vector<bool> want) {
+    ctx->save_for_backward({g, x, a, b});
+    for (int i = 0; i < 3; ++i) ctx->saved_data["r" + std::to_string(i)] = static_cast<bool>(want[i]);
+    at::AutoDispatchBelowAutograd guard;
+    if (any_cuda({g, x, a, b}) && !any_traced({g, x, a, b})) {
+      /* Gradients come back already reduced to the inputs' shapes; an
+         unwanted output skips its work (only ∂x skips the fraction). */
+      return defined_or_zero(
+          run_reduced_backward(tsb_incomplete_beta_backward, "incomplete_beta_backward", g, {x, a, b}, want),
+          {x, a, b});
+    }
+    static auto op = c10::Dispatcher::singleton()
+                         .findSchemaOrThrow("torchscience::incomplete_beta_backward", "")
+                         .typed<T3i(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&)>();
+    auto [gx, ga, gb] = op.call(g, x, a, b);
+    return {gx, ga, gb};
+  }
+  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
+    auto saved = ctx->get_saved_variables();
+    bool any_req = false, any_go = false;
+    for (int i = 0; i < 3; ++i) {
+      any_req = any_req || ctx->saved_data["r" + std::to_string(i)].toBool();
+      any_go = any_go || go[i].defined();
+    }
+    variable_list none(5);
+    if (!any_go || !any_req) return none;
+    at::AutoDispatchBelowAutograd guard;
+    at::Tensor gg[3];
+    for (int i = 0; i < 3; ++i) gg[i] = go[i].defined() ? go[i] : at::zeros_like(saved[1 + i]);
+    static auto op = c10::Dispatcher::singleton()
+                         .findSchemaOrThrow("torchscience::incomplete_beta_backward_backward", "")
+                         .typed<T4i(const at::Tensor&, const at::Tensor&, const at::Tensor&, const at::Tensor&,
+                                    const at::Tensor&, const at::Tensor&, const at::Tensor&)>();
+    auto [gg_out, g_x, g_a, g_b] = op.call(gg[0], gg[1], gg[2], saved[0], saved[1], saved[2], saved[3]);
+    return {gg_out, g_x, g_a, g_b, at::Tensor()};
+  }
+};
+
+class IncompleteBeta : public torch::autograd::Function<IncompleteBeta> {
+ public:
+  static at::Tensor forward(AutogradContext* ctx, const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+    ctx->save_for_backward({x, a, b});
+    const at::Tensor* in[3] = {&x, &a, &b};
+    for (int i = 0; i < 3; ++i) ctx->saved_data["r" + std::to_string(i)] = wants_grad(*in[i]);
+    at::AutoDispatchBelowAutograd guard;
+    static auto op = c10::Dispatcher::singleton()
+                         .findSchemaOrThrow("torchscience::incomplete_beta", "")
+                         .typed<at::Tensor(const at::Tensor&, const at::Tensor&, const at::Tensor&)>();
+    return op.call(x, a, b);
+  }
+  static variable_list backward(AutogradContext* ctx, const variable_list& go) {
+    auto saved = ctx->get_saved_variables();
+    std::vector<bool> want(3);
+    for (int i = 0; i < 3; ++i) want[i] = ctx->saved_data["r" + std::to_string(i)].toBool();
+    auto g = IncompleteBetaBackward::apply(go[0], saved[0], saved[1], saved[2], want);
+    variable_list out(3);
+    for (int i = 0; i < 3; ++i) out[i] = want[i] ? g[i] : at::Tensor();
+    return out;
+  }
+};
+
+at::Tensor ibeta_autograd(const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+  return IncompleteBeta::apply(x, a, b);
+}
+at::Tensor ibeta_autocast(const at::Tensor& x, const at::Tensor& a, const at::Tensor& b) {
+  c10::impl::ExcludeDispatchKeyGuard no_autocast(c10::DispatchKey::AutocastCUDA);
+  const auto t = at::autocast::promote_type(at::kFloat, c10::DeviceType::CUDA, x, a, b);
+  static auto op = c10::Dispatcher::singleton()
+                       .findSchemaOrThrow("torchscience::incomplete_beta", "")
+                       .typed<at::Tensor(const at::Tensor&, const at::Tensor&, const at::Tensor&)>();
+  const auto dev = c10::DeviceType::CUDA;
+  return op.call(at::autocast::cached_cast(t, x, dev), at::autocast::cached_cast(t, a, dev),
+                 at::autocast::cached_cast(t, b, dev));
+}
+}  // namespace tsbh::ops
+
+TORCH_LIBRARY_IMPL(torchscience, CUDA, m) {
+  m.impl("incomplete_beta", tsbh::ops::ibeta_cuda);
+  m.impl("incomplete_beta_backward", tsbh::ops::ibeta_backward_cuda);
+  m.impl("incomplete_beta_backward_backward", tsbh::ops::ibeta_backward_backward_cuda);
+}
+TORCH_LIBRARY_IMPL(torchscience, Meta, m) {
+  m.impl("incomplete_beta", tsbh::ops::ibeta_meta);
+  m.impl("incomplete_beta_backward", tsbh::ops::ibeta_backward_meta);
+  m.impl("incomplete_beta_backward_backward", tsbh::ops::ibeta_backward_backward_meta);
+}
+TORCH_LIBRARY_IMPL(torchscience, CPU, m) {
+  m.impl("incomplete_beta", tsbh::ops::ibeta_cpu);
+  m.impl("incomplete_beta_backward", tsbh::ops::ibeta_backward_cpu);
+  m.impl("incomplete_beta_backward_backward", tsbh::ops::ibeta_backward_backward_cpu);
+}
+TORCH_LIBRARY_IMPL(torchscience, Autograd, m) { m.impl("incomplete_beta", tsbh::ops::ibeta_autograd); }
+TORCH_LIBRARY_IMPL(torchscience, AutocastCUDA, m) { m.impl("incomplete_beta", tsbh::ops::ibeta_autocast); }
+
 // ------------------------------------------- probability callers of P and Q
 // gamma / chi2 / poisson cumulative distributions, the chi2 survival function
 // and the gamma / chi2 densities (torchscience.cpp:1881-1924).  As in the

@@ -121,6 +121,13 @@
   (m).def(                                                                                                             \
       "spherical_bessel_k_backward_backward(Tensor gg_n, Tensor gg_z, Tensor grad_output, Tensor n, Tensor z) -> "     \
       "(Tensor, Tensor, Tensor)");                                                                                     \
+  /* torchscience.cpp:833-835 */                                                                                     \
+  (m).def("incomplete_beta(Tensor x, Tensor a, Tensor b) -> Tensor");                                                \
+  (m).def(                                                                                                           \
+      "incomplete_beta_backward(Tensor grad_output, Tensor x, Tensor a, Tensor b) -> (Tensor, Tensor, Tensor)");     \
+  (m).def(                                                                                                           \
+      "incomplete_beta_backward_backward(Tensor gg_x, Tensor gg_a, Tensor gg_b, Tensor grad_output, Tensor x, "      \
+      "Tensor a, Tensor b) -> (Tensor, Tensor, Tensor, Tensor)");                                                    \
   /* torchscience.cpp:837-839 */                                                                                     \
   (m).def("hypergeometric_2_f_1(Tensor a, Tensor b, Tensor c, Tensor z) -> Tensor");                                 \
   (m).def(                                                                                                           \

@@ -153,6 +153,16 @@ def beta(a: Tensor, b: Tensor) -> Tensor:
     return torch.ops.torchscience.beta(a, b)
 
 
+def incomplete_beta(z: Tensor, a: Tensor, b: Tensor) -> Tensor:
+    """Regularized incomplete beta function I_z(a, b) for 0 < z < 1 and
+    a, b > 0: 0 for z <= 0, 1 for z >= 1, NaN for a <= 0 or b <= 0.
+    Differentiable in z, a and b (to second order); the a/b derivatives are
+    exact to rounding.  Same signature as the reference wrapper
+    (src/torchscience/special_functions/_incomplete_beta.py:5).
+    """
+    return torch.ops.torchscience.incomplete_beta(z, a, b)
+
+
 def bessel_j_1(z: Tensor) -> Tensor:
     """Bessel function of the first kind of order one, J_1(z) (odd in z).
 
@@ -322,6 +332,7 @@ __all__ = [
     "digamma",
     "gamma",
     "hypergeometric_2_f_1",
+    "incomplete_beta",
     "log_beta",
     "log_gamma",
     "modified_bessel_i",
