@@ -683,6 +683,76 @@ def secondary_arm(args):
                 with torch.no_grad():
                     res[f"{name}_{tag}_fwd_gelem_s"] = _rate(lambda: fn(mm), mm.numel(), S, W, flush)
                 res[f"{name}_{tag}_fwd_bwd_gelem_s"] = _rate(fb, mm.numel(), S, W, flush)
+    elif args.workload == "siblings":
+        n = 1 << 24
+        desc = ("the ops beside P and Q, FP64, 2^24 elements each: incomplete_beta (x ~ U(0, 1), a, b ~ "
+                "LogU(0.05, 300)), log_beta and beta (a, b ~ LogU(1e-3, 1e6)), polygamma (n ~ U{0..30}, "
+                "z ~ LogU(1e-3, 1e3)), bessel_j_1 / bessel_y_0 / modified_bessel_k_1 and spherical_bessel_j_0 "
+                "(z ~ LogU(1e-3, 1e3)), spherical_bessel_j (n ~ U(0, 20)), chi2_cumulative_distribution and "
+                "gamma_probability_density (x ~ LogU(1e-3, 1e3), df / shape ~ LogU(0.1, 100), scale 1); fwd, and "
+                "fwd + all gradients by autograd; the reference's compiled scalar kernels on 2^14 of the same "
+                "elements over all host threads (fwd, and fwd + its backward op)")
+        from torchscience_b200 import probability as pr
+
+        z = LU(n, 1e-3, 1e3)
+        cases = {
+            "incomplete_beta": (sf.incomplete_beta, [U(n, 0.0, 1.0), LU(n, 0.05, 300.0), LU(n, 0.05, 300.0)], 3),
+            "log_beta": (sf.log_beta, [LU(n, 1e-3, 1e6), LU(n, 1e-3, 1e6)], 2),
+            "beta": (sf.beta, [LU(n, 1e-3, 1e6), LU(n, 1e-3, 1e6)], 2),
+            "polygamma": (sf.polygamma, [torch.floor(U(n, 0.0, 31.0)), z], 2),
+            "bessel_j_1": (sf.bessel_j_1, [z], 1),
+            "bessel_y_0": (sf.bessel_y_0, [z], 1),
+            "modified_bessel_k_1": (sf.modified_bessel_k_1, [z], 1),
+            "spherical_bessel_j_0": (sf.spherical_bessel_j_0, [z], 1),
+            "spherical_bessel_j": (sf.spherical_bessel_j, [U(n, 0.0, 20.0), z], 2),
+            "chi2_cumulative_distribution": (pr.chi2_cumulative_distribution, [z, LU(n, 0.1, 100.0)], 2),
+            "gamma_probability_density": (pr.gamma_probability_density,
+                                          [z, LU(n, 0.1, 100.0), torch.ones(n, device=dev, dtype=torch.float64)], 3),
+        }
+        ref_cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                import time
+
+                import numpy as np
+
+                from oracle import oracle as O
+
+                if O.reference_available():
+                    ref_cpu = (O, np, time)
+            except Exception:
+                ref_cpu = None
+        for name, (fn, ins, n_in) in cases.items():
+            row = {}
+            with torch.no_grad():
+                row["fwd_gelem_s"] = _rate(lambda: fn(*ins), n, S, W, flush)
+            req = [t.clone().requires_grad_(True) for t in ins]
+            if name == "polygamma":
+                req[0] = ins[0]  # the order is not differentiable
+            gout = torch.ones(n, device=dev, dtype=torch.float64)
+            wrt = [t for t in req if t.requires_grad]
+
+            def fb():
+                torch.autograd.grad(fn(*req), wrt, gout)
+
+            row["fwd_bwd_gelem_s"] = _rate(fb, n, S, W, flush)
+            if ref_cpu is not None:
+                O, np, time = ref_cpu
+                m = 1 << 14
+                sample = [t[:m].cpu().numpy() for t in ins]
+                key = {"chi2_cumulative_distribution": "chi2_cumulative_distribution",
+                       "gamma_probability_density": "gamma_probability_density"}.get(name, name)
+                t0 = time.perf_counter()
+                O.reference(key, 0, *sample)
+                t1 = time.perf_counter()
+                O.reference(key, 1, np.ones(m), *sample)
+                t2 = time.perf_counter()
+                row["reference_cpu_fwd_gelem_s"] = m / (t1 - t0) / 1e9
+                row["reference_cpu_fwd_bwd_gelem_s"] = m / ((t2 - t0)) / 1e9
+                row["gpu_over_reference_cpu_fwd_bwd"] = row["fwd_bwd_gelem_s"] / row["reference_cpu_fwd_bwd_gelem_s"]
+            res[name] = row
+        if ref_cpu is not None:
+            res["reference_cpu_threads"] = os.cpu_count()
     print(json.dumps({
         "metric": METRIC, "workload": args.workload, "unit": "Gelem/s", "steps": S, "warmup": W,
         "data": "synthetic, seeded on the device", "config": {"workload": desc, "l2": "flushed between steps"},
@@ -697,8 +767,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument(
-        "--workload", choices=["p_grid", "c1", "c3", "c4", "c5"], default="p_grid",
-        help="p_grid (default): the headline P(a, x) workload; c1/c3/c4/c5: the other configurations, one GPU")
+        "--workload", choices=["p_grid", "c1", "c3", "c4", "c5", "siblings"], default="p_grid",
+        help="p_grid (default): the headline P(a, x) workload; c1/c3/c4/c5: the other configurations, one GPU; "
+             "siblings: the ops beside P and Q, one GPU")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
