@@ -123,3 +123,40 @@ def test_hyp2f1_reference_accuracy_bands():
     assert np.median(e[z < 0.5]) < 1e-14
     assert e[z >= 0.95].max() > 1e-3
     assert np.median(e[z >= 0.99]) > 1e-8
+
+
+def test_incomplete_beta_fixture_pinned():
+    """The incomplete_beta fixture: mpmath truth against scipy's betainc
+    (an independent implementation) and the beta density, and the
+    reference's own outputs stored beside them within the reference's
+    accuracy (its fraction stops at 200 terms, so a, b >= 300 are left out)."""
+    import scipy.special as sp
+    import scipy.stats as st
+
+    d = golden("incomplete_beta")
+    x, a, b = d["x"], d["a"], d["b"]
+    np.testing.assert_allclose(d["truth_v"], sp.betainc(a, b, x), rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(d["truth_dx"], st.beta.pdf(x, a, b), rtol=1e-10, atol=1e-300)
+    small = (a < 300) & (b < 300)
+    np.testing.assert_allclose(d["ref"][small], d["truth_v"][small], rtol=0, atol=1e-11)
+
+
+def test_incomplete_beta_known_answers_from_reference_tests():
+    """The reference's own known answers (incomplete_beta_test.cpp:70-114):
+    I_z(1, 1) = z, I_z(1, b) = 1 - (1-z)^b, I_z(a, 1) = z^a and
+    I_z(a, b) + I_(1-z)(b, a) = 1, checked on the stored mpmath truth's
+    generator (scipy here) and on the reference's compiled kernel where built."""
+    import scipy.special as sp
+
+    from oracle import oracle as O
+
+    z = np.array([0.1, 0.25, 0.5, 0.75, 0.9])
+    np.testing.assert_allclose(sp.betainc(1.0, 3.0, z), 1 - (1 - z) ** 3, rtol=1e-13)
+    np.testing.assert_allclose(sp.betainc(3.0, 1.0, z), z**3, rtol=1e-13)
+    if not O.reference_available():
+        pytest.skip("reference library not built")
+    (u,) = O.reference("incomplete_beta", 0, np.array([0.0, 0.25, 0.5, 0.75, 1.0]), 1.0, 1.0)
+    np.testing.assert_allclose(u, [0.0, 0.25, 0.5, 0.75, 1.0], atol=1e-12)
+    (s1,) = O.reference("incomplete_beta", 0, z, 2.5, 3.5)
+    (s2,) = O.reference("incomplete_beta", 0, 1 - z, 3.5, 2.5)
+    np.testing.assert_allclose(s1 + s2, 1.0, atol=1e-10)

@@ -144,3 +144,27 @@ def test_gradcheck():
     b = (torch.rand(6, dtype=torch.float64, device="cuda") * 4 + 0.5).requires_grad_()
     assert torch.autograd.gradcheck(sf.incomplete_beta, (x, a, b), eps=1e-6, atol=1e-7, rtol=1e-6)
     assert torch.autograd.gradgradcheck(sf.incomplete_beta, (x, a, b), eps=1e-6, atol=1e-6, rtol=1e-5)
+
+
+def test_known_answers_from_reference_tests():
+    """The reference's known answers (incomplete_beta_test.cpp:70-114,
+    test__incomplete_beta.py:118-215): I_z(1, 1) = z, I_z(1, b) = 1 - (1-z)^b,
+    I_z(a, 1) = z^a, I_z(a, b) + I_(1-z)(b, a) = 1, 0 at z = 0 and 1 at z = 1,
+    at the reference's tolerances or tighter."""
+    z = torch.tensor([0.0, 0.25, 0.5, 0.75, 1.0], dtype=torch.float64, device="cuda")
+    one = torch.ones_like(z)
+    torch.testing.assert_close(sf.incomplete_beta(z, one, one), z, rtol=0, atol=1e-15)
+    z = torch.tensor([0.1, 0.25, 0.3, 0.5, 0.7, 0.75, 0.9], dtype=torch.float64, device="cuda")
+    for v in (0.5, 2.0, 3.0, 7.5):
+        c = torch.full_like(z, v)
+        torch.testing.assert_close(sf.incomplete_beta(z, torch.ones_like(z), c), 1 - (1 - z) ** v, rtol=1e-14, atol=1e-15)
+        torch.testing.assert_close(sf.incomplete_beta(z, c, torch.ones_like(z)), z**v, rtol=1e-14, atol=1e-15)
+    for a, b in ((2.5, 3.5), (0.3, 12.0), (40.0, 0.7)):
+        A, B = torch.full_like(z, a), torch.full_like(z, b)
+        s = sf.incomplete_beta(z, A, B) + sf.incomplete_beta(1 - z, B, A)
+        torch.testing.assert_close(s, torch.ones_like(z), rtol=0, atol=4e-16 * 4)
+    for a, b in ((0.5, 0.5), (2.0, 3.0), (100.0, 0.1)):
+        A = torch.full((2,), a, dtype=torch.float64, device="cuda")
+        B = torch.full((2,), b, dtype=torch.float64, device="cuda")
+        e = torch.tensor([0.0, 1.0], dtype=torch.float64, device="cuda")
+        assert sf.incomplete_beta(e, A, B).tolist() == [0.0, 1.0]
