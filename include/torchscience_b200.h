@@ -157,8 +157,11 @@ TSB_OP_SIGNATURE(tsb_regularized_gamma_q_backward_backward);
  * TSB_NOALLOC_SCRATCH_BYTES that each GPU loading the library keeps until
  * exit; requests needing more return TSB_ERR_WORKSPACE without launching.
  * The first call on a device looks up the array's address and should come
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race and must be serialized by the caller. */
+ * before any stream capture.  The address is cached per device for the life
+ * of the process: after cudaDeviceReset (which unloads this library's device
+ * code with the context) the entry point must not be called again in that
+ * process.  All calls share the array: calls that overlap on the GPU race
+ * and must be serialized by the caller. */
 #define TSB_NOALLOC_SCRATCH_BYTES (8ll << 20)
 int32_t tsb_regularized_gamma_p_backward_noalloc(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out,
                                                  int32_t n_out, int32_t precision, void* stream);

@@ -9,11 +9,13 @@
                                   accelerated ops (oracle/ref_ops.cpp), for the
                                   reference arm of bench.py.
 
-The two _ref libraries are built only when the reference sources are present
-(REFERENCE_ROOT, default /root/reference); they are git-ignored build products.
-Nothing is written outside oracle/.
+The two _ref libraries are built from the reference checkout named by the
+REFERENCE_ROOT environment variable; with it unset (or pointing at no
+sources) they are not rebuilt, a message says so, and any existing build is
+kept.  They are git-ignored build products.  Nothing is written outside
+oracle/.
 
-Usage: python oracle/build_ref.py [--force]
+Usage: REFERENCE_ROOT=<reference checkout> python oracle/build_ref.py [--force]
 """
 
 from __future__ import annotations
@@ -26,8 +28,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent
-REF_ROOT = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
-REF_CSRC = REF_ROOT / "src" / "torchscience" / "csrc"
+REF_ROOT = Path(os.environ["REFERENCE_ROOT"]) if os.environ.get("REFERENCE_ROOT") else None
+REF_CSRC = REF_ROOT / "src" / "torchscience" / "csrc" if REF_ROOT else None
 OUT = HERE / "_ref"
 
 
@@ -65,8 +67,12 @@ def build_restatement(force=False) -> Path:
 
 
 def build_reference(force=False) -> list[Path]:
-    if not REF_CSRC.is_dir():
-        return []
+    if REF_CSRC is None or not REF_CSRC.is_dir():
+        have = [p for p in (OUT / "libref_scalar.so", OUT / "libtorchscience_ref.so") if p.exists()]
+        why = "REFERENCE_ROOT is unset" if REF_CSRC is None else f"no reference sources under {REF_ROOT}"
+        sys.stderr.write(f"oracle/build_ref.py: {why}; oracle/_ref not rebuilt"
+                         f" ({len(have)} existing librar{'y' if len(have) == 1 else 'ies'} kept)\n")
+        return have
     OUT.mkdir(exist_ok=True)
     _, incs, libdir, abi = _torch()
     common = ["-std=c++17", "-fPIC", "-shared", "-fopenmp", f"-I{REF_CSRC}", f"-D_GLIBCXX_USE_CXX11_ABI={abi}"]

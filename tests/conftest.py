@@ -21,3 +21,14 @@ def pytest_collection_modifyitems(config, items):
     for item in items:
         if "gpu" in item.keywords:
             item.add_marker(skip)
+
+
+@pytest.fixture(autouse=True)
+def _seed_default_generators():
+    """Every test starts from the same state of torch's default generators
+    (CPU and every CUDA device), whatever ran before it, so a test that draws
+    from them without its own generator sees the same values in any order."""
+    import torch
+
+    torch.manual_seed(0)
+    yield

@@ -59,6 +59,27 @@ def test_noalloc_matches_the_workspace_entry_point_on_two_calls(dtype, tol):
             assert torch.allclose(got.double(), want.double(), rtol=tol, atol=tol * scale), f"call {call}"
 
 
+@pytest.mark.parametrize("layout", ["scalar_a", "full_shape"])
+def test_noalloc_other_layouts(layout):
+    """A scalar a reduces its gradient over the whole grid (one partial per
+    tile in the scratch array); full-shape a and x need no scratch at all."""
+    a, x, g = inputs(2, 300, 517, torch.float64)
+    if layout == "scalar_a":
+        a = a[:1, :1].clone()  # (1, 1): broadcast along both dimensions
+    else:
+        a, x = a.expand(g.shape).contiguous(), x.expand(g.shape).contiguous()
+    for call in range(2):
+        want_a, want_x = run("regularized_gamma_p_backward", g, a, x, n_out=2, out_shapes=[a.shape, x.shape])
+        ga = torch.full_like(a, float("nan"))
+        gx = torch.full_like(x, float("nan"))
+        st = noalloc(g, a, x, ga, gx)
+        assert st == 0, f"call {call}: {lib().tsb_last_error().decode()}"
+        torch.cuda.synchronize()
+        for got, want in ((ga, want_a), (gx, want_x)):
+            scale = want.double().abs().max().item()
+            assert torch.allclose(got.double(), want.double(), rtol=1e-12, atol=1e-12 * scale), f"call {call}"
+
+
 def test_noalloc_rejects_requests_beyond_its_scratch():
     # 70000 rows x 4096 columns: the row-reduced partials alone need
     # 128 column tiles x 70000 rows x 8 bytes, far above 8 MiB.  The upstream

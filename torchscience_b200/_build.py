@@ -52,13 +52,32 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError(f"command failed ({proc.returncode}): {' '.join(cmd[:6])} ...")
 
 
+def _deps_of(obj: Path):
+    """Headers the unit included when `obj` was last compiled (the compiler's
+    -MD dependency file beside it), or None when there is no such record."""
+    dfile = obj.with_suffix(".d")
+    if not dfile.exists():
+        return None
+    text = dfile.read_text().replace("\\\n", " ")
+    _, _, rest = text.partition(":")
+    return [Path(t) for t in rest.split()]
+
+
 def _compile_units(units, out_dir: Path, compile_fn, deps_mtime: float, force: bool, jobs: int):
+    """Compiles each unit whose object is missing or older than the unit or
+    any header it included (from its dependency file; without one, older
+    than any header of the tree, `deps_mtime`)."""
     out_dir.mkdir(parents=True, exist_ok=True)
     todo, objs = [], []
     for src in units:
         obj = out_dir / (src.stem + ".o")
         objs.append(obj)
-        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, deps_mtime):
+        deps = _deps_of(obj) if obj.exists() else None
+        if deps is None or not all(d.exists() for d in deps):
+            newest = deps_mtime
+        else:
+            newest = _newest(deps)
+        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest):
             todo.append((src, obj))
     if todo:
         with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -74,9 +93,13 @@ def build_kernels(force: bool = False, jobs: int | None = None) -> Path:
     deps = _newest(list(KERNELS.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
 
     def cc(src, obj):
-        _run([NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+        _run([NVCC, *NVCC_FLAGS, "-MD", "-MF", str(obj.with_suffix(".d")), "-c", str(src), "-o", str(obj)])
 
     objs, changed = _compile_units(units, BUILD / "kernels", cc, deps, force, jobs)
+    for stale in (BUILD / "kernels").glob("*.o"):
+        if stale not in objs:  # a unit that was removed or renamed
+            stale.unlink()
+            stale.with_suffix(".d").unlink(missing_ok=True)
     if changed or force or not KERNEL_LIB.exists() or KERNEL_LIB.stat().st_mtime < _newest(objs):
         _run([NVCC, *ARCH_FLAGS, "-shared", "-o", str(KERNEL_LIB), *map(str, objs), "-Xcompiler", "-fPIC"])
     return KERNEL_LIB
@@ -114,7 +137,8 @@ def build_ops(force: bool = False, jobs: int | None = None) -> Path:
     deps = _newest(list(HOST.glob("*.h")) + list(INCLUDE.glob("*.h")))
 
     def cc(src, obj):
-        _run(["g++", "-O2", "-std=c++17", "-fPIC", *cflags, "-c", str(src), "-o", str(obj)])
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", *cflags, "-MD", "-MF", str(obj.with_suffix(".d")), "-c", str(src),
+              "-o", str(obj)])
 
     objs, changed = _compile_units(units, BUILD / "host", cc, deps, force, jobs)
     if changed or force or not OPS_LIB.exists() or OPS_LIB.stat().st_mtime < max(_newest(objs), KERNEL_LIB.stat().st_mtime):

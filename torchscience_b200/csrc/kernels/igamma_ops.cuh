@@ -134,7 +134,11 @@ struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
 };
 
 // Backward from kept derivatives: in = {grad, d_a, d_b}, out = {grad·d_a,
-// grad·d_b}, each reduced to its input's shape by the 2-D kernel.
+// grad·d_b}, each reduced to its input's shape by the 2-D kernel.  The
+// products are formed in double for every storage type (GradProductD), so
+// a reduced gradient of float data is rounded once, after the sum, as the
+// reference's backward op rounds each product once
+// (regularized_gamma_p_backward.h:27-33).
 template <typename T_>
 struct GradProduct {
   using T = T_;
@@ -146,6 +150,7 @@ struct GradProduct {
   }
 };
 
+template <typename T> using GradProductD = GradProduct<double>;
 template <typename T> using GammaPFwd = IgammaFwd<T, false>;
 template <typename T> using GammaPBwd = IgammaBwd<T, false>;
 template <typename T> using GammaPBwdBwd = IgammaBwdBwd<T, false>;

@@ -4,4 +4,4 @@
 
 TSB_DEFINE_OP(tsb_regularized_gamma_p_forward_with_grads, tsb::GammaPFwdGrad)
 TSB_DEFINE_OP(tsb_regularized_gamma_q_forward_with_grads, tsb::GammaQFwdGrad)
-TSB_DEFINE_OP(tsb_gradient_product, tsb::GradProduct)
+TSB_DEFINE_OP(tsb_gradient_product, tsb::GradProductD)

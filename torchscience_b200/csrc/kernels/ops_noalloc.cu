@@ -15,7 +15,9 @@
 // Rules that follow from the shared array:
 //   - the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before any stream capture;
+//     that first call before any stream capture.  The cache lives as long as
+//     the process: cudaDeviceReset destroys the context that holds the array,
+//     so after a reset this entry point must not be called again;
 //   - every call uses the same array, so calls that overlap on the GPU (on
 //     different streams, or from different host threads) race and must be
 //     serialized by the caller;
