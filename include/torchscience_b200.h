@@ -19,6 +19,13 @@
  *     double, in a fixed order).  This is how backward kernels return
  *     gradients already reduced to an input's shape.  Reduced outputs need a
  *     device workspace of tsb_workspace_bytes(...) bytes.
+ *   - a grid of an (R, 1) input against a (1, C) input (or the transpose)
+ *     also asks for a small workspace (tsb_workspace_bytes > 0 even with no
+ *     reduced output): the incomplete-gamma entry points use it to evaluate
+ *     the grid in rows sorted by the shape parameter (one warp per 32 sorted
+ *     rows), which keeps the lanes of a warp on the same code path.  Without
+ *     it (workspace NULL or too small, no reduced output) they run the
+ *     unsorted tile kernel and give the same values.
  *   - an output whose `data` is NULL is not requested and is not computed.
  *   - all operands of one call have the same dtype.
  *   - precision: TSB_PRECISION_AUTO picks the FP64 kernels for f64 data and

@@ -80,10 +80,15 @@ def test_workspace_query_for_the_broadcast_grid():
     ga = desc(shape, strides=[1, 0])
     gx = desc(shape, strides=[0, 1])
     n = L.tsb_workspace_bytes(arr(g, a, x), 3, arr(ga, gx), 2)
-    # row-reduced: 128 column tiles x 4096 rows; column-reduced: 128 row tiles (32 rows) x 4096 cols (doubles)
-    assert n == (128 + 128) * 4096 * 8
-    # no reduced output -> 0
-    assert L.tsb_workspace_bytes(arr(g, a, x), 3, arr(desc(shape), desc(shape)), 2) == 0
+    # row-reduced: 128 column tiles x 4096 rows; column-reduced: 128 row tiles (32 rows) x 4096 cols (doubles);
+    # then the row-sorted sweep's scratch: the row order (4096 int32), row and column tables (16 doubles per
+    # row and per column) and the task counter (256 bytes)
+    sweep = 4096 * 4 + (4096 + 4096) * 16 * 8 + 256
+    assert n == (128 + 128) * 4096 * 8 + sweep
+    # no reduced output: only the sweep's scratch on an (R, 1) x (1, C) grid
+    assert L.tsb_workspace_bytes(arr(g, a, x), 3, arr(desc(shape), desc(shape)), 2) == sweep
+    # ... and nothing for a layout without a row-constant and a column-constant input
+    assert L.tsb_workspace_bytes(arr(g, g, g), 3, arr(desc(shape), desc(shape)), 2) == 0
 
 
 def test_reduced_layout_needing_three_dims_is_reported():

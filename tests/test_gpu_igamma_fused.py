@@ -139,3 +139,33 @@ def test_derivatives_are_kept_only_for_a_recorded_forward():
         y = sf.regularized_gamma_p(ar, xr)
         plain = torch.cuda.memory_allocated() - m1
     assert kept >= 3 * size and plain < 2 * size
+
+
+@pytest.mark.parametrize("layout", ["grid", "contiguous"])
+def test_recompute_strategy(layout):
+    """autograd_strategy("recompute"): the forward keeps nothing and the
+    backward evaluates the derivatives again (reduced in the same pass); its
+    gradients equal the kept-derivative ones."""
+    if layout == "grid":
+        a, x = inputs((300, 1), (1, 500), seed=6)
+    else:
+        a, x = inputs((40000,), (40000,), seed=7)
+    g = randn(torch.broadcast_shapes(a.shape, x.shape), torch.float64, seed=13)
+    grads = {}
+    for strategy in ("keep", "recompute"):
+        with torchscience_b200.autograd_strategy(strategy):
+            ar, xr = a.clone().requires_grad_(True), x.clone().requires_grad_(True)
+            torch.cuda.synchronize()
+            m0 = torch.cuda.memory_allocated()
+            y = sf.regularized_gamma_p(ar, xr)
+            held = torch.cuda.memory_allocated() - m0
+            grads[strategy] = torch.autograd.grad(y, (ar, xr), g)
+            if strategy == "recompute":
+                assert held < 2 * y.numel() * 8, held
+    with torch.no_grad():
+        ta, tx = torch.ops.torchscience.regularized_gamma_p_backward(g.abs(), a, x)
+    for got, want, terms in zip(grads["recompute"], grads["keep"], (ta, tx)):
+        scale = terms.double().abs().sum_to_size(got.shape)
+        worst = ((got - want).abs() / (scale + 1e-300)).max().item()
+        assert worst <= 1e-13, f"recompute vs keep: worst |difference| / sum |terms| = {worst:.3g}"
+    assert torchscience_b200.get_autograd_strategy() == "keep"

@@ -26,7 +26,14 @@ if not (_os.path.exists(KERNEL_LIBRARY) and _os.path.exists(OPS_LIBRARY)):
 _torch.ops.load_library(OPS_LIBRARY)
 
 from . import probability, special_functions  # noqa: E402
-from ._precision import get_precision_mode, precision, set_precision_mode  # noqa: E402
+from ._precision import (  # noqa: E402
+    autograd_strategy,
+    get_autograd_strategy,
+    get_precision_mode,
+    precision,
+    set_autograd_strategy,
+    set_precision_mode,
+)
 
 __all__ = [
     "probability",
@@ -34,6 +41,9 @@ __all__ = [
     "set_precision_mode",
     "get_precision_mode",
     "precision",
+    "set_autograd_strategy",
+    "get_autograd_strategy",
+    "autograd_strategy",
     "KERNEL_LIBRARY",
     "OPS_LIBRARY",
 ]

@@ -84,20 +84,33 @@ def call(name: str, inputs, outputs, precision: int = 0, workspace: torch.Tensor
     return fn(din, len(inputs), dout, len(outputs), precision, ws, ctypes.c_int64(wsb), stream)
 
 
-def run(name: str, *inputs, n_out: int = 1, precision: int = 0, out_shapes=None) -> list[torch.Tensor]:
-    """Broadcast call through the C ABI; outputs full-shape unless out_shapes given (reduced)."""
+def sweep_scratch_bytes(shape) -> int:
+    """Bytes of the workspace that only the row-sorted sweep of a 2-D grid
+    uses (its row order, row and column tables of 16 doubles per entry, and
+    task counter): the last part of what tsb_workspace_bytes asks for on such
+    a grid."""
+    n0, n1 = (shape[-2], shape[-1]) if len(shape) >= 2 else (0, 0)
+    return ((max(n0, n1) * 4 + 255) & ~255) + (((n0 + n1) * 16 * 8 + 255) & ~255) + 256
+
+
+def run(name: str, *inputs, n_out: int = 1, precision: int = 0, out_shapes=None, sweep: bool = True) -> list[torch.Tensor]:
+    """Broadcast call through the C ABI; outputs full-shape unless out_shapes
+    given (reduced).  The workspace is the one tsb_workspace_bytes asks for;
+    with sweep=False it is cut short of the sweep's scratch (none at all when
+    no output is reduced), so a 2-D grid runs the unsorted tile kernel."""
     shape = torch.broadcast_shapes(*[t.shape for t in inputs])
     outs = []
     for k in range(n_out):
         s = shape if out_shapes is None or out_shapes[k] is None else out_shapes[k]
         outs.append(torch.empty(s, dtype=inputs[0].dtype, device=inputs[0].device))
-    ws = None
-    if out_shapes is not None:
-        din = (TsbTensor * len(inputs))(*[describe(t, shape) for t in inputs])
-        dout = (TsbTensor * n_out)(*[describe(o, shape) for o in outs])
-        nbytes = lib().tsb_workspace_bytes(din, len(inputs), dout, n_out)
-        assert nbytes >= 0, lib().tsb_last_error()
-        ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=inputs[0].device)
+    din = (TsbTensor * len(inputs))(*[describe(t, shape) for t in inputs])
+    dout = (TsbTensor * n_out)(*[describe(o, shape) for o in outs])
+    nbytes = lib().tsb_workspace_bytes(din, len(inputs), dout, n_out)
+    assert nbytes >= 0, lib().tsb_last_error()
+    reduced = out_shapes is not None and any(s is not None and tuple(s) != tuple(shape) for s in out_shapes)
+    if not sweep and nbytes > 0:
+        nbytes = nbytes - sweep_scratch_bytes(shape) if reduced else 0
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=inputs[0].device) if nbytes > 0 else None
     st = call(name, list(inputs), outs, precision=precision, workspace=ws, shape=shape)
     assert st == 0, f"tsb_{name} -> {st}: {lib().tsb_last_error().decode()}"
     return outs

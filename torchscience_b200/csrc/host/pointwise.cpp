@@ -46,6 +46,20 @@ void check_status(int32_t st, const char* name) {
   TORCH_CHECK(st == TSB_OK, "torchscience_b200 ", name, ": ", tsb_status_string(st), ": ", tsb_last_error());
 }
 
+// Calls `fn` with the workspace the C ABI asks for (none for most layouts;
+// for a (R, 1) x (1, C) grid, the row order of the sorted sweep), taken from
+// the caching allocator on the current stream.
+void call_with_workspace(OpFn fn, const char* name, std::vector<tsb_tensor>& din, std::vector<tsb_tensor>& dout,
+                         const at::TensorOptions& opts, cudaStream_t stream) {
+  const int64_t ws = tsb_workspace_bytes(din.data(), (int32_t)din.size(), dout.data(), (int32_t)dout.size());
+  check_status(ws < 0 ? (int32_t)ws : TSB_OK, name);
+  at::Tensor workspace;
+  if (ws > 0) workspace = at::empty({ws}, opts.dtype(at::kByte));
+  check_status(fn(din.data(), (int32_t)din.size(), dout.data(), (int32_t)dout.size(), precision_mode().load(),
+                  ws > 0 ? workspace.data_ptr() : nullptr, ws, stream),
+               name);
+}
+
 }  // namespace
 
 [[noreturn]] void cpu_not_supported(const char* name) {
@@ -136,7 +150,7 @@ std::vector<at::Tensor> run_pointwise(OpFn fn, const char* name, at::TensorList 
     return res;
   }
   const auto stream = c10::cuda::getCurrentCUDAStream(dev.index()).stream();
-  check_status(fn(din.data(), n_in, dout.data(), n_out, precision_mode().load(), nullptr, 0, stream), name);
+  call_with_workspace(fn, name, din, dout, res[0].options(), stream);
   return res;
 }
 
@@ -237,8 +251,7 @@ std::vector<at::Tensor> run_pointwise_masked(OpFn fn, const char* name, at::Tens
   for (const auto& t : ins) din.push_back(describe(t, full));
   for (int o = 0; o < n_out; ++o) dout.push_back(want[o] ? describe(res[o], full) : describe(at::Tensor(), full, false));
   const auto stream = c10::cuda::getCurrentCUDAStream(dev.index()).stream();
-  check_status(fn(din.data(), (int32_t)din.size(), dout.data(), n_out, precision_mode().load(), nullptr, 0, stream),
-               name);
+  call_with_workspace(fn, name, din, dout, opts, stream);
   return res;
 }
 

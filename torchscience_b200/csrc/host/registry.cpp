@@ -20,6 +20,15 @@ using torch::autograd::variable_list;
 
 namespace tsbh {
 
+// Whether autograd's forward of regularized_gamma_p / _q keeps the first
+// derivatives (one evaluation; 16 bytes per element of float64 output stay
+// alive until the backward) or the backward evaluates them again from the
+// inputs (no extra memory).  Process-wide; on by default.
+inline std::atomic<bool>& keep_derivatives() {
+  static std::atomic<bool> keep{true};
+  return keep;
+}
+
 inline bool wants_grad(const at::Tensor& t) {
   return t.requires_grad() && (at::isFloatingType(t.scalar_type()) || at::isComplexType(t.scalar_type()));
 }
@@ -319,7 +328,7 @@ inline torch::autograd::variable_list defined_or_zero(std::vector<at::Tensor> r,
       ctx->saved_data["ra"] = ra;                                                                               \
       ctx->saved_data["rb"] = rb;                                                                               \
       at::AutoDispatchBelowAutograd guard;                                                                      \
-      if ((ra || rb) && recorded && any_cuda({a, b}) && !any_traced({a, b})) {                                 \
+      if ((ra || rb) && recorded && keep_derivatives().load() && any_cuda({a, b}) && !any_traced({a, b})) {    \
         auto r = run_pointwise_masked(FWDGRAD, #name, {a, b}, 3, {true, ra, rb});                               \
         ctx->save_for_backward({a, b, r[1], r[2]});                                                             \
         ctx->saved_data["fused"] = true;                                                                        \
@@ -830,11 +839,15 @@ int64_t set_precision_mode(int64_t mode) {
   return precision_mode().exchange(static_cast<int>(mode));
 }
 int64_t get_precision_mode() { return precision_mode().load(); }
+bool set_keep_derivatives(bool keep) { return keep_derivatives().exchange(keep); }
+bool get_keep_derivatives() { return keep_derivatives().load(); }
 std::string library_version() { return tsb_version(); }
 }  // namespace tsbh
 
 TORCH_LIBRARY(torchscience_b200, m) {
   m.def("set_precision_mode(int mode) -> int", &tsbh::set_precision_mode);
   m.def("get_precision_mode() -> int", &tsbh::get_precision_mode);
+  m.def("set_keep_derivatives(bool keep) -> bool", &tsbh::set_keep_derivatives);
+  m.def("get_keep_derivatives() -> bool", &tsbh::get_keep_derivatives);
   m.def("version() -> str", &tsbh::library_version);
 }

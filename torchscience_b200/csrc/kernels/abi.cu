@@ -92,10 +92,22 @@ int64_t tsb_workspace_bytes(const tsb_tensor* in, int32_t n_in, const tsb_tensor
   bool reduced = false;
   for (int o = 0; o < n_out; ++o)
     if (out[o].data && tsb::output_is_reduced(c, n_in + o)) reduced = true;
-  if (!reduced) return 0;
+  // A 2-D grid with an input constant along each dimension ((R, 1) x (1, C)):
+  // room for the row-sorted sweep's row order, row and column tables and
+  // task counter, which the functions with per-input tables use when given.
+  int64_t sweep = 0;
+  if (c.numel > 0 && c.ndim == 2) {
+    bool row_const = false, col_const = false;
+    for (int k = 0; k < n_in; ++k) {
+      row_const |= c.stride[k][0] != 0 && c.stride[k][1] == 0;
+      col_const |= c.stride[k][0] == 0 && c.stride[k][1] != 0;
+    }
+    if (row_const && col_const) sweep = tsb::sweep_scratch_bytes(c.size[0], c.size[1]);
+  }
+  if (!reduced) return sweep;
   if (c.ndim > 2)
     return tsb::set_error(TSB_ERR_LAYOUT, "reduced outputs need an iteration space of at most 2 coalesced dims");
-  return tsb::reduce_ws_bytes(c, n_in, out, n_out, tsb::kTRMin);
+  return tsb::reduce_ws_bytes(c, n_in, out, n_out, tsb::kTRMin) + sweep;
 }
 
 }  // extern "C"

@@ -10,6 +10,7 @@
 #include <algorithm>
 
 #include "map.cuh"
+#include "sweep_decl.cuh"
 
 namespace tsb {
 
@@ -173,6 +174,8 @@ template <class Fn, typename TS>
 struct MapTag {};
 template <class Fn, typename TS>
 struct ReduceTag {};
+template <class Fn, typename TS, int PASS>
+struct SweepTag {};
 
 inline int32_t check_launch(const char* what) {
   const cudaError_t e = cudaGetLastError();
@@ -229,6 +232,26 @@ int32_t launch_reduce(const Canon& c, const tsb_tensor* in, const tsb_tensor* ou
   }
   return TSB_OK;
 }
+
+// Sweep layout: input ia constant along one dimension and varying along the
+// other, input ix the reverse.  Sets `transpose` when ia varies along the
+// columns (the problem is then swept with rows and columns exchanged).
+inline bool sweep_layout(const Canon& c, int ia, int ix, bool& transpose) {
+  if (c.ndim != 2) return false;
+  const int64_t a0 = c.stride[ia][0], a1 = c.stride[ia][1], x0 = c.stride[ix][0], x1 = c.stride[ix][1];
+  if (a0 != 0 && a1 == 0 && x0 == 0 && x1 != 0) transpose = false;
+  else if (a0 == 0 && a1 != 0 && x0 != 0 && x1 == 0) transpose = true;
+  else return false;
+  return c.size[transpose ? 1 : 0] <= kSweepMaxRows;
+}
+
+// Runs Fn through the row-sorted sweep; defined in sweep.cuh, which the
+// units of functors with SWEEP include.  Returns TSB_ERR_WORKSPACE without
+// launching when `ws` is too small for the partial sums and the sweep's
+// scratch, so that the caller can fall back to the tile kernel.
+template <class Fn, typename TS>
+int32_t launch_sweep(const Canon& c, bool transpose, const tsb_tensor* out, uint32_t mask, const tsb_tensor* in,
+                     void* ws, int64_t ws_bytes, cudaStream_t stream, int dev, const DeviceInfo* info);
 
 template <int NIN, int NOUT>
 inline void fill_map_params(const Canon& c, const tsb_tensor* in, const tsb_tensor* out, uint32_t mask,
@@ -332,6 +355,24 @@ int32_t run_op(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_
     if ((mask & (1u << o)) && output_is_reduced(c, NIN + o)) reduced = true;
   cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
   const bool use64 = precision == TSB_PRECISION_FP64;
+  if constexpr (HasAux<FD>::value && SweepOptIn<FD>::value) {
+    // (R, 1) x (1, C) grids (or the transpose) with a workspace: the
+    // row-sorted sweep.  Without room for its scratch, the tile kernel below.
+    bool tr = false;
+    if (ws && sweep_layout(c, FD::AUX_IN0, FD::AUX_IN1, tr)) {
+      int32_t sw = TSB_ERR_DTYPE;
+      switch (dtype) {
+        case TSB_F64: sw = launch_sweep<FD, double>(c, tr, out, mask, in, ws, ws_bytes, s, dev, info); break;
+        case TSB_F32:
+          sw = use64 ? launch_sweep<FD, float>(c, tr, out, mask, in, ws, ws_bytes, s, dev, info)
+                     : launch_sweep<FF, float>(c, tr, out, mask, in, ws, ws_bytes, s, dev, info);
+          break;
+        case TSB_F16: sw = launch_sweep<FF, __half>(c, tr, out, mask, in, ws, ws_bytes, s, dev, info); break;
+        case TSB_BF16: sw = launch_sweep<FF, __nv_bfloat16>(c, tr, out, mask, in, ws, ws_bytes, s, dev, info); break;
+      }
+      if (sw != TSB_ERR_WORKSPACE) return sw;
+    }
+  }
   if constexpr (HasAux<FD>::value) {
     // A 2-D grid on which an input with per-row/column tables is broadcast
     // runs through the tiled 2-D kernel (every output full), which builds the

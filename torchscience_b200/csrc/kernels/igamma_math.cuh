@@ -538,18 +538,145 @@ __device__ inline IgammaOut igamma_eval_mf(int region, float a, float x, const I
   return o;
 }
 
+// exp(v)·m in float, for ln-values v (float-float) whose exponential is
+// below the normal range: expf is taken at v + 64 and the product scaled by
+// e^-64 last, so a subnormal result is rounded once.
+__device__ __forceinline__ float ff_exp_mul(IgFF v, float m) {
+  if (v.hi > -80.0f) return expf(v.hi) * (1.0f + v.lo) * m;
+  return (expf(v.hi + 64.0f) * (1.0f + v.lo) * m) * 1.60381089e-28f;
+}
+
+// Regions whose first derivatives the mixed kernels evaluate in FP32 (bit r
+// for region r); the others, and every second derivative, run in FP64.
+// Measured against the FP64 kernels on the 4096 x 4096 benchmark grid (max
+// relative error of P, ∂P/∂a, ∂P/∂x): the series regions up to x < 0.7 (a+1)
+// stay below 5e-7; kIgS3 reaches 3e-6, the float continued fraction's
+// a-derivative 1.4e-6 (kIgC0) to 5.5e-6 (kIgC2); kIgSmallA 1.5e-6 where
+// ln x > ψ(a+1) (those elements take FP64).  The fraction regions run in
+// FP32 only through the large-x expansion (igamma_asym_f, x >= 20).
+#ifndef TSB_IG_FP32_MASK1
+#define TSB_IG_FP32_MASK1 ((1u << kIgS00) | (1u << kIgS0) | (1u << kIgS1) | (1u << kIgS2) | (1u << kIgC00) | \
+                           (1u << kIgC0) | (1u << kIgSmallA0) | (1u << kIgSmallA))
+#endif
+
+// Γ(a,x) x^(1-a) e^x = Σ_{k>=0} (a-1)(a-2)...(a-k) / x^k, the large-x
+// expansion (DLMF 8.11.2), in float, with its a-derivative: t_k = t_{k-1}
+// (a-k)/x and dt_k/da = (dt_{k-1}/da)(a-k)/x + t_{k-1}/x, products only.
+// For x >= 20 and x >= 3(a+1) the terms fall below 3e-8 of the sum within
+// about 15 terms (they shrink by (a-k)/x <= 1/3 while k < a, and by at most
+// k/x beyond, the smallest being ~2e-8 at x = 20); an integer a ends the
+// value's series exactly.  The derivative enters ∂Q/∂a as E1 S + S1 with S ~ 1
+// and E1 = ln x - ψ(a) >= ~2.5 here, so its terms are judged against
+// dscale = E1, not against S1 (~1/x), whose own relative accuracy does not
+// matter.  The loop also stops at the smallest term once the terms grow (the
+// expansion diverges beyond k ~ x + a).
+__device__ inline void igamma_asym_f(float a, float x, float dscale, float& S, float& S1) {
+  const float rx = 1.0f / x;
+  float t = 1.0f, dt = 0.0f;
+  S = 1.0f;
+  S1 = 0.0f;
+  for (int k = 1; k <= 48; ++k) {
+    const float f = (a - (float)k) * rx;
+    if ((float)k > a && fabsf(f) >= 1.0f) break;  // terms would grow
+    dt = fmaf(dt, f, t * rx);
+    t *= f;
+    S += t;
+    S1 += dt;
+    if (fabsf(t) <= 3e-8f * S && fabsf(dt) <= 3e-8f * dscale) break;
+  }
+}
+
+// Mixed evaluation of P (or Q) with ∂P/∂a and ∂P/∂x, entirely in FP32, for
+// float data in the regions of TSB_IG_FP32_MASK1.
+//   ln D = a ln x - x - lnΓ(a+1) (a < 10) or a (ln x - ln a) - (x - a) - C(a)
+//   in float-float from the double per-row / per-column quantities, exact to
+//   ~1e-11 absolute even where the terms cancel;
+//   series (x < a+1):  P = D S,  ∂P/∂a = D (L1 S + S1),  L1 = ln x - ψ(a+1);
+//   fraction:          Q = E F,  ∂Q/∂a = E (E1 F + F1),  E = D a,
+//                      E1 = ln x - ψ(a) (L1 and E1 in float-float from the
+//                      tables, so their cancellation near x ~ a costs nothing);
+//   ∂P/∂x = D a / x = E / x from its logarithm, in range wherever the result is.
+// In the series region L1 S and S1 have the same sign for x <= a and nearly
+// so up to a + 1, and in the fraction region E1 > 0 and F1 > 0: the
+// derivative sums do not cancel.  Q in the series region (and P in the
+// fraction region) is 1 - the other, in double.  Small a with Q requested
+// keeps the FP64 small-a formula (the caller routes it there).
+template <bool WANT_Q>
+__device__ inline IgammaOut igamma_eval_mf1(int region, float a, float x, const IgPre& P) {
+  IgammaOut o;
+  o.paa = o.pax = o.pxx = 0.0;
+  const IgFF lx = P.lxff(), lg = P.lgff(), la = P.laff();
+  IgFF lnD;
+  if (a < 10.0f) {
+    lnD = ff_add(ff_add(ff_mul_f(lx, a), IgFF{-x, 0.0f}), ff_neg(lg));
+  } else {
+    const IgFF d = ff_add(lx, ff_neg(la));
+    lnD = ff_add(ff_add(ff_mul_f(d, a), ff_neg(ff_two_sum(x, -a))), ff_neg(lg));
+  }
+  const IgFF lnE = ff_add(lnD, la);
+  const IgFF lnEx = ff_add(lnE, ff_neg(lx));  // ln(E/x) = ln ∂P/∂x
+  o.px = ff_exp_mul(lnEx, 1.0f);
+  if (region == kIgC0 || region == kIgC00) {
+    // Q = (E/x) S, ∂Q/∂a = (E/x) (E1 S + S1), E1 = ln x - ψ(a) (x >= 20 here)
+    float S, S1;
+    const IgFF E1 = ff_add(lx, ff_neg(P.psff()));
+    igamma_asym_f(a, x, fabsf(E1.hi), S, S1);
+    const float qv = ff_exp_mul(lnEx, S);
+    o.q = qv;
+    o.p = 1.0 - (double)qv;
+    o.pa = -(double)ff_exp_mul(lnEx, fmaf(E1.hi, S, fmaf(E1.lo, S, S1)));
+  } else if (region != kIgC1 && region != kIgC2) {
+    float S, S1, S2;
+    igamma_series<float, 1>(a, x, S, S1, S2);
+    const IgFF L1 = ff_add(lx, ff_neg(P.prff()));
+    const float pv = ff_exp_mul(lnD, S);
+    o.p = pv;
+    o.q = 1.0 - (double)pv;
+    o.pa = ff_exp_mul(lnD, fmaf(L1.hi, S, fmaf(L1.lo, S, S1)));
+  } else {
+    float F, F1, F2;
+    igamma_cf<float, 1>(a, x, F, F1, F2);
+    const IgFF E1 = ff_add(lx, ff_neg(P.psff()));
+    const float qv = ff_exp_mul(lnE, F);
+    o.q = qv;
+    o.p = 1.0 - (double)qv;
+    o.pa = -(double)ff_exp_mul(lnE, fmaf(E1.hi, F, fmaf(E1.lo, F, F1)));
+  }
+  return o;
+}
+
+// Whether the mixed kernels evaluate (a, x) of `region` with its first
+// derivatives in FP64: regions outside TSB_IG_FP32_MASK1; the small-a Q;
+// ln x > ψ(a+1) in kIgSmallA (there L1 S and S1 have opposite signs); the
+// fraction regions below x = 20 (the expansion needs x >= 20).
+__device__ __forceinline__ bool igamma_needs_fp64_1(int region, float xf, const IgPre& P, bool want_q) {
+  return region == kIgSpecial || !((TSB_IG_FP32_MASK1 >> region) & 1u) ||
+         (want_q && (region == kIgSmallA || region == kIgSmallA0)) ||
+         (region == kIgSmallA && P.lxf() > P.prff().hi) || ((region == kIgC0 || region == kIgC00) && !(xf >= 20.0f));
+}
+
+// The FP64 evaluation with first derivatives as one out-of-line function,
+// for the mixed kernels' FP64 regions.
+template <bool WANT_Q>
+__device__ __noinline__ IgammaOut igamma_eval_d1_call(float a, float x, const IgPre P) {
+  return igamma_eval_d<1, WANT_Q>((double)a, (double)x, P);
+}
+
 // Evaluation for float data.  P or Q alone (ORDER 0): FP32 in the light
 // regions (igamma_eval_mf), FP64 elsewhere: the heavy regions (large a near
 // the transition x ~ a, where the term count grows like √a and float
-// accumulation would exceed 1e-6) and the small-a Q.  Derivatives (ORDER >= 1)
-// are evaluated in FP64 throughout: the a-derivative of the continued
-// fraction and of the longer series loses ~1e-5 in FP32, and a kernel holding
-// both precisions' code paths measured slower than the FP64 one (instruction
-// fetch) on the 4096 x 4096 grid.
+// accumulation would exceed 1e-6) and the small-a Q.  First derivatives
+// (ORDER 1): FP32 in the regions of TSB_IG_FP32_MASK1 (igamma_eval_mf1), FP64
+// elsewhere.  Second derivatives: FP64.
 template <int ORDER, bool WANT_Q = false>
 __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf, const IgPre& P) {
-  if constexpr (ORDER >= 1) {
+  if constexpr (ORDER >= 2) {
     return igamma_eval_d<ORDER, WANT_Q>((double)af, (double)xf, P);
+  } else if constexpr (ORDER == 1) {
+    // The FP64 evaluator is one out-of-line copy (igamma_eval_d1_call), so
+    // the inline code is the FP32 path.
+    if (igamma_needs_fp64_1(region, xf, P, WANT_Q)) return igamma_eval_d1_call<WANT_Q>(af, xf, P);
+    return igamma_eval_mf1<WANT_Q>(region, af, xf, P);
   } else {
     if (region == kIgSmallA || region == kIgSmallA0) {
       if (WANT_Q) return igamma_eval_d<0, true>((double)af, (double)xf, P);

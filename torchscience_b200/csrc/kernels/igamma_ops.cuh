@@ -7,6 +7,7 @@
 
 #include "dispatch.cuh"
 #include "igamma_math.cuh"
+#include "sweep.cuh"
 
 // Resident CTAs the forward's register allocation must allow (64 registers).
 #ifndef TSB_IGF_MINB
@@ -35,6 +36,7 @@ template <int ORDER, int IA, int IX, typename T>
 struct IgammaAuxIO {
   static constexpr int AUX_IN0 = IA, AUX_IN1 = IX;
   static constexpr int NAUX0 = kIgAuxA, NAUX1 = kIgAuxX;
+  static constexpr bool SWEEP = true;  // (R, 1) x (1, C) grids run the row-sorted sweep
   __device__ static void make_aux0(T v, double* o) { igamma_aux_a<ORDER>((double)v, o); }
   __device__ static void make_aux1(T v, double* o) { igamma_aux_x((double)v, o); }
   __device__ static IgPre pre(const T* in, const double* A, const double* X) {
@@ -80,6 +82,32 @@ struct IgammaBwd : IgammaAuxIO<1, 1, 2, T_> {
     out[0] = (T)(sgn * g * o.pa);
     out[1] = (T)(sgn * g * o.px);
   }
+  // Two-pass sweep of float data: pass 1 the FP32 elements, pass 2 the rest.
+  static constexpr bool SPLIT = sizeof(T) == 4;
+  __device__ static bool fp64_pass(int r, const T* in, uint32_t mask, const double* A, const double* X) {
+    return !(mask & 1u) || r == kIgSat0 || r == kIgSat1 ||
+           igamma_needs_fp64_1(r, (float)in[2], IgammaBwd::pre(in, A, X), false);
+  }
+  template <int PASS>
+  __device__ static void eval_pass(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
+    const double sgn = UPPER ? -1.0 : 1.0;
+    const double g = in[0];
+    const IgPre P = IgammaBwd::pre(in, A, X);
+    if constexpr (PASS == 1) {
+      const IgammaOut o = igamma_eval_mf1<false>(r, (float)in[1], (float)in[2], P);
+      out[0] = (T)(sgn * g * o.pa);
+      out[1] = (T)(sgn * g * o.px);
+    } else {
+      if (!(mask & 1u)) {
+        out[0] = T(0);
+        out[1] = (T)(sgn * g * igamma_px_only((double)in[1], (double)in[2], P));
+        return;
+      }
+      const IgammaOut o = igamma_eval<1>(r, (double)in[1], (double)in[2], P);
+      out[0] = (T)(sgn * g * o.pa);
+      out[1] = (T)(sgn * g * o.px);
+    }
+  }
 };
 
 template <typename T_, bool UPPER>
@@ -92,9 +120,12 @@ struct IgammaBwdBwd : IgammaAuxIO<2, 3, 4, T_> {
     const double sgn = UPPER ? -1.0 : 1.0;
     const double gga = in[0], ggx = in[1], g = in[2];
     const IgammaOut o = igamma_eval<2>(r, in[3], in[4], IgammaBwdBwd::pre(in, A, X));
-    out[0] = (T)(sgn * (gga * o.pa + ggx * o.px));
-    out[1] = (T)(sgn * g * (gga * o.paa + ggx * o.pax));
-    out[2] = (T)(sgn * g * (gga * o.pax + ggx * o.pxx));
+    // sums of two products as explicit fmas, so that every kernel that
+    // instantiates this functor rounds them the same way (the compiler may
+    // otherwise contract either product)
+    out[0] = (T)(sgn * fma(gga, o.pa, __dmul_rn(ggx, o.px)));
+    out[1] = (T)(sgn * g * fma(gga, o.paa, __dmul_rn(ggx, o.pax)));
+    out[2] = (T)(sgn * g * fma(gga, o.pax, __dmul_rn(ggx, o.pxx)));
   }
 };
 
@@ -119,14 +150,43 @@ struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
                               const double* X = nullptr) {
     const double sgn = UPPER ? -1.0 : 1.0;
     const IgPre P = IgammaFwdGrad::pre(in, A, X);
+    // in[] are T: float data takes the mixed evaluators (igamma_eval_m)
     if (!(mask & 2u)) {
-      const IgammaOut o = igamma_eval<0, UPPER>(r, (double)in[0], (double)in[1], P);
+      const IgammaOut o = igamma_eval<0, UPPER>(r, in[0], in[1], P);
       out[0] = (T)(UPPER ? o.q : o.p);
       out[1] = T(0);
       out[2] = (T)(sgn * igamma_px_only((double)in[0], (double)in[1], P));
       return;
     }
-    const IgammaOut o = igamma_eval<1, UPPER>(r, (double)in[0], (double)in[1], P);
+    const IgammaOut o = igamma_eval<1, UPPER>(r, in[0], in[1], P);
+    out[0] = (T)(UPPER ? o.q : o.p);
+    out[1] = (T)(sgn * o.pa);
+    out[2] = (T)(sgn * o.px);
+  }
+  // Two-pass sweep of float data: pass 1 the FP32 elements (compact FP32
+  // code alone in its kernel), pass 2 the rest in FP64.
+  static constexpr bool SPLIT = sizeof(T) == 4;
+  __device__ static bool fp64_pass(int r, const T* in, uint32_t mask, const double* A, const double* X) {
+    return !(mask & 2u) || r == kIgSat0 || r == kIgSat1 ||
+           igamma_needs_fp64_1(r, (float)in[1], IgammaFwdGrad::pre(in, A, X), UPPER);
+  }
+  template <int PASS>
+  __device__ static void eval_pass(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
+    const double sgn = UPPER ? -1.0 : 1.0;
+    const IgPre P = IgammaFwdGrad::pre(in, A, X);
+    IgammaOut o;
+    if constexpr (PASS == 1) {
+      o = igamma_eval_mf1<UPPER>(r, (float)in[0], (float)in[1], P);
+    } else {
+      if (!(mask & 2u)) {
+        o = igamma_eval<0, UPPER>(r, (double)in[0], (double)in[1], P);
+        out[0] = (T)(UPPER ? o.q : o.p);
+        out[1] = T(0);
+        out[2] = (T)(sgn * igamma_px_only((double)in[0], (double)in[1], P));
+        return;
+      }
+      o = igamma_eval<1, UPPER>(r, (double)in[0], (double)in[1], P);
+    }
     out[0] = (T)(UPPER ? o.q : o.p);
     out[1] = (T)(sgn * o.pa);
     out[2] = (T)(sgn * o.px);
