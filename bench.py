@@ -661,19 +661,54 @@ def secondary_arm(args):
     def LU(n, lo, hi, dtype=torch.float64):
         return torch.exp(U(n, math.log(lo), math.log(hi))).to(dtype)
 
+    ref = None
+    if not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, ROOT)
+            from oracle import oracle as O
+
+            if O.reference_available():
+                ref = O
+        except Exception:
+            ref = None
+
+    def roofline(bytes_per_elem, gelem_s, kernel):
+        achieved = bytes_per_elem * gelem_s
+        return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": peak_src,
+                "unit": "GB/s", "frac": achieved / peak, "algorithmic_bytes_per_elem": bytes_per_elem}
+
+    def cpu(calls, n_sample, what):
+        """The reference's compiled scalar kernels (oracle/_ref) over a sample of
+        the same inputs on all host threads: Gelem/s of the same step."""
+        if ref is None:
+            return None
+        calls()  # warm
+        t0 = time.perf_counter()
+        calls()
+        dt = time.perf_counter() - t0
+        return {"value": n_sample / dt / 1e9, "unit": "Gelem/s", "cores": ref.threads(), "kind": "reference",
+                "sample": f"{n_sample} elements of the same inputs; {what}"}
+
+    def np_(t, m):
+        return t[:m].double().cpu().numpy()
+
     if args.workload == "c1":
-        desc = "log_gamma and bessel_j_0 FP64 forward, x ~ U(0.01, 50), contiguous"
+        desc = "log_gamma and bessel_j_0 FP64 forward, x ~ U(0.01, 50), contiguous (2^20, the configuration; 2^28)"
         for n in (1 << 20, 1 << 28):
             x = U(n, 0.01, 50.0)
             for name in ("log_gamma", "bessel_j_0"):
                 fn = getattr(sf, name)
                 r = _rate(lambda: fn(x), n, S, W, flush)
-                res[f"{name}_2^{int(math.log2(n))}"] = {
-                    "fwd_gelem_s": r, "hbm_gbs": 16 * r, "hbm_frac": 16 * r / peak}
+                row = {"fwd_gelem_s": r, "roofline": roofline(16, r, f"{name} forward (map kernel), float64")}
+                if n == 1 << 20:
+                    xs = np_(x, n)
+                    row["cpu_baseline"] = cpu(lambda: ref.reference(name, 0, xs), n, "forward, float64")
+                res[f"{name}_2^{int(math.log2(n))}"] = row
             del x
     elif args.workload == "c3":
         n = 1 << 26
-        desc = "bessel J/Y/I/K, nu ~ U(0, 20), x ~ LogU(1e-3, 1e3), 2^26 elements; fwd and fwd + d/dx"
+        desc = ("bessel J/Y/I/K, nu ~ U(0, 20), x ~ LogU(1e-3, 1e3), 2^26 elements; fwd and fwd + d/dx "
+                "(float32 data: the mixed kernels; float64: the FP64 kernels on the same values)")
         nu64, x64 = U(n, 0.0, 20.0), LU(n, 1e-3, 1e3)
         nu32, x32 = nu64.float(), x64.float()
         g32 = torch.randn(n, generator=gen, device=dev, dtype=torch.float32)
@@ -693,6 +728,13 @@ def secondary_arm(args):
             with torch.no_grad():
                 row["mixed_max_rel_err_vs_fp64"] = _max_rel(fn(nu32, x32), fn(nu32.double(), x32.double()))
             row["mixed_speedup_fwd_bwd"] = row["mixed_fwd_bwd_gelem_s"] / row["fp64_fwd_bwd_gelem_s"]
+            # fwd + d/dx: read nu, x, g, write y and grad_x (4 B each in float32, 8 in float64)
+            row["roofline_mixed"] = roofline(20, row["mixed_fwd_bwd_gelem_s"], f"{name} fwd + backward, float32")
+            row["roofline_fp64"] = roofline(40, row["fp64_fwd_bwd_gelem_s"], f"{name} fwd + backward, float64")
+            m = 1 << 13
+            nn, xx, gg = np_(nu32, m), np_(x32, m), np_(g32, m)
+            row["cpu_baseline"] = cpu(lambda: (ref.reference(name, 0, nn, xx), ref.reference(name, 1, gg, nn, xx)),
+                                      m, "forward + backward (the reference's backward op), float64")
             res[name] = row
         del nu64, x64, nu32, x32, g32
         # 2^20 points within relative 1e-6 of the first 100 zeros of J0 (ν = 0) and J1 (ν = 1)
@@ -739,9 +781,19 @@ def secondary_arm(args):
             with torch.no_grad():
                 res[f"{tag}_fwd_gelem_s"] = _rate(lambda: sf.hypergeometric_2_f_1(*ins), n, S, W, flush)
             res[f"{tag}_fwd_bwd_gelem_s"] = _rate(fb, n, S, W, flush)
+        # fwd: 4 inputs + 1 output; bwd: g + 4 inputs read, 4 grads written (8 B each in float64)
+        res["roofline_fp64"] = roofline(40 + 72, res["fp64_fwd_bwd_gelem_s"], "2F1 fwd + backward, float64")
+        res["roofline_mixed"] = roofline(20 + 36, res["mixed_fwd_bwd_gelem_s"], "2F1 fwd + backward, float32")
+        m = 1 << 11
+        an, bn, cn, zn, gn = (np_(t, m) for t in (a, b, c, z, g))
+        res["cpu_baseline"] = cpu(lambda: (ref.reference("hypergeometric_2_f_1", 0, an, bn, cn, zn),
+                                           ref.reference("hypergeometric_2_f_1", 1, gn, an, bn, cn, zn)),
+                                  m, "forward + backward (the reference's backward op), float64")
     elif args.workload == "c5":
+        from torchscience_b200 import probability as pr
+
         desc = ("Gamma log-likelihood sum over 2^28 elements, k ~ LogU(0.1, 100), theta ~ LogU(0.1, 10), "
-                "x ~ Gamma(k, theta); fwd + grads (autograd) + HVP in k (double backward); "
+                "x ~ Gamma(k, theta): value + grads in k and theta (one fused pass) + HVP in k (fused); "
                 "K(m), E(m), m ~ U(0, 1 - 1e-9), 2^26 elements, fwd + d/dm")
         n = 1 << 28
         k, th = LU(n, 0.1, 100.0, torch.float32), LU(n, 0.1, 10.0, torch.float32)
@@ -750,21 +802,49 @@ def secondary_arm(args):
         v = torch.randn(n, generator=gen, device=dev, dtype=torch.float32)
         for tag, dt in (("mixed", torch.float32), ("fp64", torch.float64)):
             kk, tt, xx, vv = (t.to(dt) for t in (k, th, x, v))
-            kr, tr = kk.clone().requires_grad_(True), tt.clone().requires_grad_(True)
 
             def step():
-                L = ((kr - 1) * torch.log(xx) - xx / tr - sf.log_gamma(kr) - kr * torch.log(tr)).sum()
-                gk, gt = torch.autograd.grad(L, (kr, tr), create_graph=True)
-                torch.autograd.grad(gk, kr, vv)
+                pr.gamma_log_likelihood_value_and_grad(xx, kk, tt, (False, True, True))
+                pr.gamma_log_likelihood_hvp(xx, kk, tt, None, vv, None, out_mask=(False, True, False))
 
-            res[f"likelihood_{tag}_fwd_bwd_hvp_gelem_s"] = _rate(step, n, S, W, flush)
-            del kk, tt, xx, vv, kr, tr
+            r = _rate(step, n, S, W, flush)
+            res[f"likelihood_{tag}_fwd_bwd_hvp_gelem_s"] = r
+            # fused value + gradients: read x, k, theta, write grad_k, grad_theta (20 B/elem in float32);
+            # HVP in k: read x, k, theta, v, write one (20 B more)
+            eb = 4 if dt == torch.float32 else 8
+            res[f"likelihood_{tag}_roofline"] = roofline(10 * eb, r, f"gamma log-likelihood value+grad+HVP, {tag}")
+            if tag == "mixed":
+                kr, tr = kk.clone().requires_grad_(True), tt.clone().requires_grad_(True)
+
+                def autograd_step():
+                    L = pr.gamma_log_likelihood(xx, kr, tr)
+                    gk, gt = torch.autograd.grad(L, (kr, tr), create_graph=True)
+                    torch.autograd.grad(gk, kr, vv)
+
+                res["likelihood_mixed_through_autograd_gelem_s"] = _rate(autograd_step, n, S, W, flush)
+                del kr, tr
+            del kk, tt, xx, vv
             torch.cuda.empty_cache()
+        m = 1 << 18
+        xs, ks, ts, vs = (np_(t, m) for t in (x, k, th, v))
+
+        def ref_step():
+            import numpy as np
+
+            (lg,) = ref.reference("log_gamma", 0, ks)
+            L = np.sum((ks - 1) * np.log(xs) - xs / ts - lg - ks * np.log(ts))
+            (dk,) = ref.reference("log_gamma", 1, np.ones_like(ks), ks)  # psi(k)
+            gk, gt = np.log(xs) - dk - np.log(ts), xs / ts**2 - ks / ts
+            ref.reference("log_gamma", 2, vs, np.ones_like(ks), ks)  # psi'(k) v
+            return L, gk, gt
+
+        res["likelihood_cpu_baseline"] = cpu(ref_step, m, "the reference's log_gamma, its backward (psi) and "
+                                             "double backward (psi') with numpy for the rest, float64")
         del k, th, x, v
-        m = U(1 << 26, 0.0, 1.0 - 1e-9, torch.float32)
+        mm32 = U(1 << 26, 0.0, 1.0 - 1e-9, torch.float32)
         for name in ("complete_legendre_elliptic_integral_k", "complete_legendre_elliptic_integral_e"):
             fn = getattr(sf, name)
-            for tag, mm in (("mixed", m), ("fp64", m.double())):
+            for tag, mm in (("mixed", mm32), ("fp64", mm32.double())):
                 mr = mm.clone().requires_grad_(True)
 
                 def fb():
@@ -774,6 +854,14 @@ def secondary_arm(args):
                 with torch.no_grad():
                     res[f"{name}_{tag}_fwd_gelem_s"] = _rate(lambda: fn(mm), mm.numel(), S, W, flush)
                 res[f"{name}_{tag}_fwd_bwd_gelem_s"] = _rate(fb, mm.numel(), S, W, flush)
+                eb = 4 if tag == "mixed" else 8
+                # fwd: read m, write K; fwd + bwd: + read g, write dK/dm
+                res[f"{name}_{tag}_roofline"] = roofline(4 * eb, res[f"{name}_{tag}_fwd_bwd_gelem_s"],
+                                                         f"{name} fwd + backward, {tag}")
+            ms = np_(mm32, 1 << 16)
+            res[f"{name}_cpu_baseline"] = cpu(lambda: (ref.reference(name, 0, ms),
+                                                       ref.reference(name, 1, ms * 0 + 1, ms)),
+                                              1 << 16, "forward + backward, float64")
     elif args.workload == "siblings":
         n = 1 << 24
         desc = ("the ops beside P and Q, FP64, 2^24 elements each: incomplete_beta (x ~ U(0, 1), a, b ~ "

@@ -96,6 +96,15 @@ int64_t tsb_workspace_bytes(const tsb_tensor* in, int32_t n_in, const tsb_tensor
  * the reference, whose operators run on the CPU). */
 int64_t tsb_launch_count(void);
 
+/* Number of elements, since the last reset, whose series, continued fraction
+ * or recurrence stopped at its iteration cap on the current device (their
+ * results are truncated sums: every loop is bounded, so such inputs cost
+ * time, never a hang).  Waits for the device to finish its work first.
+ * reset != 0 zeroes the counters after reading them.  Negative: a
+ * tsb_status.  The reference stops its loops at fixed caps too
+ * (regularized_gamma_p.h:12,30: max_iter = 200) without reporting it. */
+int64_t tsb_unconverged_count(int32_t reset);
+
 /* Every op entry point has this signature. */
 #define TSB_OP_SIGNATURE(name)                                               \
   int32_t name(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out,    \
@@ -172,6 +181,27 @@ TSB_OP_SIGNATURE(tsb_regularized_gamma_q_backward_backward);
 #define TSB_NOALLOC_SCRATCH_BYTES (8ll << 20)
 int32_t tsb_regularized_gamma_p_backward_noalloc(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out,
                                                  int32_t n_out, int32_t precision, void* stream);
+
+/* ---- Fused Gamma log-likelihood ------------------------------------------ */
+/* No single counterpart in the reference: its Gamma log-likelihood is a chain
+ * of ops around log_gamma (log_gamma.h:23-65; gradient via digamma as in
+ * kernel/probability/gamma_probability_density_backward.h:11-31; second
+ * derivatives via trigamma as in log_gamma_backward_backward.h:11-20).  Per
+ * element l = (k-1) ln x - x/theta - lnGamma(k) - k ln theta for x ~ Gamma(k, theta).
+ *
+ * tsb_gamma_log_likelihood_value_and_grad: in = {x, k, theta}; out = {L,
+ * dL/dx, dL/dk, dL/dtheta}.  L is the sum over the iteration shape (its
+ * descriptor has stride 0 in every dim), added in double in a fixed order;
+ * the gradients are per element; any output may be NULL.  One pass over the
+ * inputs.  Operands must be contiguous or broadcast scalars over the shape
+ * (TSB_ERR_LAYOUT otherwise).  Needs tsb_gamma_log_likelihood_workspace_bytes()
+ * bytes of workspace on the current device. */
+int64_t tsb_gamma_log_likelihood_workspace_bytes(void);
+TSB_OP_SIGNATURE(tsb_gamma_log_likelihood_value_and_grad);
+/* tsb_gamma_log_likelihood_hvp: in = {g, x, k, theta, u_x, u_k, u_theta}; out =
+ * the three components of g * H u per element, H the per-element Hessian of l
+ * in (x, k, theta).  Any u may be NULL (zero); any output may be NULL. */
+TSB_OP_SIGNATURE(tsb_gamma_log_likelihood_hvp);
 
 /* ---- Bessel functions --------------------------------------------------- */
 /* bessel_j_0(z): bessel_j_0.h:91-129, schema torchscience.cpp:872-874;

@@ -26,6 +26,7 @@ if not (_os.path.exists(KERNEL_LIBRARY) and _os.path.exists(OPS_LIBRARY)):
 _torch.ops.load_library(OPS_LIBRARY)
 
 from . import probability, special_functions  # noqa: E402
+from ._convergence import ConvergenceWarning, check_convergence, unconverged_count  # noqa: E402
 from ._precision import (  # noqa: E402
     autograd_strategy,
     get_autograd_strategy,
@@ -44,6 +45,9 @@ __all__ = [
     "set_autograd_strategy",
     "get_autograd_strategy",
     "autograd_strategy",
+    "unconverged_count",
+    "check_convergence",
+    "ConvergenceWarning",
     "KERNEL_LIBRARY",
     "OPS_LIBRARY",
 ]

@@ -5,6 +5,7 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "dispatch.cuh"
 
@@ -19,6 +20,23 @@ bool g_dev_init[64];
 }  // namespace
 
 void count_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+std::mutex& unconverged_mutex() {
+  static std::mutex m;
+  return m;
+}
+std::vector<int64_t (*)(bool)>& unconverged_readers() {
+  static std::vector<int64_t (*)(bool)> readers;
+  return readers;
+}
+}  // namespace
+
+bool register_unconverged_reader(int64_t (*reader)(bool reset)) {
+  std::lock_guard<std::mutex> lock(unconverged_mutex());
+  unconverged_readers().push_back(reader);
+  return true;
+}
 
 int32_t set_error(int32_t status, const char* fmt, ...) {
   char buf[512];
@@ -68,6 +86,25 @@ extern "C" {
 const char* tsb_version(void) { return "torchscience_b200 0.1.0 (sm_100a)"; }
 
 int64_t tsb_launch_count(void) { return tsb::g_launches.load(std::memory_order_relaxed); }
+
+int64_t tsb_unconverged_count(int32_t reset) {
+  int dev = 0;
+  const tsb::DeviceInfo* info = nullptr;
+  const int32_t st = tsb::current_device(&dev, &info);
+  if (st) return st;
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    const cudaError_t e = cudaGetLastError();
+    return tsb::set_error(TSB_ERR_LAUNCH, "device synchronize failed: %s", cudaGetErrorString(e));
+  }
+  std::lock_guard<std::mutex> lock(tsb::unconverged_mutex());
+  int64_t total = 0;
+  for (auto* read : tsb::unconverged_readers()) {
+    const int64_t v = read(reset != 0);
+    if (v < 0) return tsb::set_error(TSB_ERR_DEVICE, "reading a not-converged counter failed");
+    total += v;
+  }
+  return total;
+}
 
 const char* tsb_last_error(void) { return tsb::g_last_error.c_str(); }
 

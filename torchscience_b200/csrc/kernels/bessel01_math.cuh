@@ -34,6 +34,7 @@ namespace b01 {
 
 constexpr double kInvPi = 0.31830988618379067;      // 1/π
 constexpr double kInvSqrtPi = 0.56418958354775628;  // 1/sqrt(π)
+constexpr int kB01Comp = 4;                         // compensated Horner steps
 
 // UNROLL bounds how many coefficient loads are in flight (and held in
 // registers) at once.
@@ -44,8 +45,24 @@ __device__ __forceinline__ double zero_form(double x, int i) {
   const double u = (x - __ldg(&iv[i][0])) * __ldg(&iv[i][1]);
   double p = __ldg(&cf[fits::B01_DEG][i]);
 #pragma unroll UNROLL
-  for (int k = fits::B01_DEG - 1; k >= 0; --k) p = fma(p, u, __ldg(&cf[k][i]));
-  return ((x - __ldg(&iv[i][2])) - __ldg(&iv[i][3])) * p;
+  for (int k = fits::B01_DEG - 1; k >= kB01Comp; --k) p = fma(p, u, __ldg(&cf[k][i]));
+  // The last kB01Comp steps carry their rounding errors (the compensated
+  // Horner scheme of Graillat, Langlois and Louvet, 2005: the product error
+  // from an FMA, the sum error from TwoSum): their partial sums are as large
+  // as the value, so they hold most of Horner's rounding near the interval
+  // edges (|u| -> 1), where plain Horner measured up to 4 ulp.
+  double c = 0.0;
+#pragma unroll
+  for (int k = kB01Comp - 1; k >= 0; --k) {
+    const double a = __ldg(&cf[k][i]);
+    const double pu = p * u, e1 = fma(p, u, -pu);
+    const double s = pu + a, bb = s - pu, e2 = (pu - (s - bb)) + (a - bb);
+    c = fma(c, u, e1 + e2);
+    p = s;
+  }
+  // (x - z_hi) is exact near the zero (Sterbenz); (x - z_hi) - z_lo and the
+  // product round once each
+  return ((x - __ldg(&iv[i][2])) - __ldg(&iv[i][3])) * (p + c);
 }
 
 template <int N>

@@ -26,6 +26,7 @@
 // polynomial fits generated by fits/gen_fits.py.  All loops are capped.
 #pragma once
 
+#include "unconverged.cuh"
 #include <math_constants.h>
 
 #include "bessel01_math.cuh"
@@ -120,12 +121,16 @@ __device__ inline void bessel_series(T nu, T x, T sgn, T& val, T& der) {
   const T eps = BesselK<T>::EPS;
   const T h = T(0.5) * x, q = sgn * h * h;
   T t = 1, s = 1, sd = nu;
-  for (int k = 1; k < 500; ++k) {
-    t *= q / (T(k) * (nu + T(k)));
-    s += t;
-    const T td = t * (nu + T(2 * k));
-    sd += td;
-    if (fabs(t) <= eps * fabs(s) && fabs(td) <= eps * fabs(sd)) break;
+  {  // counted loop: reaching the cap is recorded (note_unconverged)
+    int k = 1;
+    for (; k < 500; ++k) {
+      t *= q / (T(k) * (nu + T(k)));
+      s += t;
+      const T td = t * (nu + T(2 * k));
+      sd += td;
+      if (fabs(t) <= eps * fabs(s) && fabs(td) <= eps * fabs(sd)) break;
+    }
+    if (k >= 500) note_unconverged();
   }
   // (x/2)^ν / Γ(ν+1): its exponent reaches a few hundred, so in the FP32
   // kernels it is formed in FP64 (an FP32 exponent would cost ~1e-5).
@@ -156,17 +161,21 @@ __device__ inline void temme_y(T mu, T x, T& ymu, T& ymu1) {
   T c = 1;
   Kahan<T> sum(ff + r * q), sum1(p);
   const T dd = -x2 * x2;
-  for (int i = 1; i < 500; ++i) {
-    const T fi = T(i);
-    ff = (fi * ff + p + q) / (fi * fi - mu * mu);
-    c *= dd / fi;
-    p /= (fi - mu);
-    q /= (fi + mu);
-    const T del = c * (ff + r * q);
-    sum.add(del);
-    const T del1 = c * p - fi * del;
-    sum1.add(del1);
-    if (fabs(del) < (T(1) + fabs(sum.s)) * eps && fabs(del1) < (T(1) + fabs(sum1.s)) * eps) break;
+  {  // counted loop: reaching the cap is recorded (note_unconverged)
+    int i = 1;
+    for (; i < 500; ++i) {
+      const T fi = T(i);
+      ff = (fi * ff + p + q) / (fi * fi - mu * mu);
+      c *= dd / fi;
+      p /= (fi - mu);
+      q /= (fi + mu);
+      const T del = c * (ff + r * q);
+      sum.add(del);
+      const T del1 = c * p - fi * del;
+      sum1.add(del1);
+      if (fabs(del) < (T(1) + fabs(sum.s)) * eps && fabs(del1) < (T(1) + fabs(sum1.s)) * eps) break;
+    }
+    if (i >= 500) note_unconverged();
   }
   ymu = -sum.s;
   ymu1 = -sum1.s * (T(2) / x);
@@ -190,17 +199,21 @@ __device__ inline void temme_k(T mu, T x, T& kmu, T& kmu1) {
   T c = 1;
   Kahan<T> sum1(p);
   const T dd = x2 * x2;
-  for (int i = 1; i < 500; ++i) {
-    const T fi = T(i);
-    ff = (fi * ff + p + q) / (fi * fi - mu * mu);
-    c *= dd / fi;
-    p /= (fi - mu);
-    q /= (fi + mu);
-    const T del = c * ff;
-    sum.add(del);
-    const T del1 = c * (p - fi * ff);
-    sum1.add(del1);
-    if (fabs(del) < fabs(sum.s) * eps && fabs(del1) < fabs(sum1.s) * eps) break;
+  {  // counted loop: reaching the cap is recorded (note_unconverged)
+    int i = 1;
+    for (; i < 500; ++i) {
+      const T fi = T(i);
+      ff = (fi * ff + p + q) / (fi * fi - mu * mu);
+      c *= dd / fi;
+      p /= (fi - mu);
+      q /= (fi + mu);
+      const T del = c * ff;
+      sum.add(del);
+      const T del1 = c * (p - fi * ff);
+      sum1.add(del1);
+      if (fabs(del) < fabs(sum.s) * eps && fabs(del1) < fabs(sum1.s) * eps) break;
+    }
+    if (i >= 500) note_unconverged();
   }
   kmu = sum.s;
   kmu1 = sum1.s * (T(2) / x);
@@ -320,17 +333,21 @@ __device__ inline JY<T> besseljy_pos(T nu, T x) {
   T h = nu * xi;
   if (h < fpmin) h = fpmin;
   T b = xi2 * nu, d = 0, c = h;
-  for (int i = 1; i < BesselK<T>::MAXIT; ++i) {
-    b += xi2;
-    d = b - d;
-    if (fabs(d) < fpmin) d = fpmin;
-    c = b - T(1) / c;
-    if (fabs(c) < fpmin) c = fpmin;
-    d = T(1) / d;
-    const T del = c * d;
-    h *= del;
-    if (d < T(0)) isign = -isign;
-    if (fabs(del - T(1)) < eps) break;
+  {  // counted loop: reaching the cap is recorded (note_unconverged)
+    int i = 1;
+    for (; i < BesselK<T>::MAXIT; ++i) {
+      b += xi2;
+      d = b - d;
+      if (fabs(d) < fpmin) d = fpmin;
+      c = b - T(1) / c;
+      if (fabs(c) < fpmin) c = fpmin;
+      d = T(1) / d;
+      const T del = c * d;
+      h *= del;
+      if (d < T(0)) isign = -isign;
+      if (fabs(del - T(1)) < eps) break;
+    }
+    if (i >= BesselK<T>::MAXIT) note_unconverged();
   }
   T rjl = T(isign) * fpmin, rjpl = h * rjl;
   T rjl1 = rjl, rjp1 = rjpl, fact = nu * xi;
@@ -361,25 +378,29 @@ __device__ inline JY<T> besseljy_pos(T nu, T x) {
   T tmp = p * dlr - q * dli;
   q = p * dli + q * dlr;
   p = tmp;
-  for (int i = 2; i < BesselK<T>::MAXIT; ++i) {
-    a += T(2 * (i - 1));
-    bi += T(2);
-    dr = a * dr + br;
-    di = a * di + bi;
-    if (fabs(dr) + fabs(di) < fpmin) dr = fpmin;
-    fct = a / (cr * cr + ci * ci);
-    cr = br + cr * fct;
-    ci = bi - ci * fct;
-    if (fabs(cr) + fabs(ci) < fpmin) cr = fpmin;
-    den = dr * dr + di * di;
-    dr /= den;
-    di /= -den;
-    dlr = cr * dr - ci * di;
-    dli = cr * di + ci * dr;
-    tmp = p * dlr - q * dli;
-    q = p * dli + q * dlr;
-    p = tmp;
-    if (fabs(dlr - T(1)) + fabs(dli) < eps) break;
+  {  // counted loop: reaching the cap is recorded (note_unconverged)
+    int i = 2;
+    for (; i < BesselK<T>::MAXIT; ++i) {
+      a += T(2 * (i - 1));
+      bi += T(2);
+      dr = a * dr + br;
+      di = a * di + bi;
+      if (fabs(dr) + fabs(di) < fpmin) dr = fpmin;
+      fct = a / (cr * cr + ci * ci);
+      cr = br + cr * fct;
+      ci = bi - ci * fct;
+      if (fabs(cr) + fabs(ci) < fpmin) cr = fpmin;
+      den = dr * dr + di * di;
+      dr /= den;
+      di /= -den;
+      dlr = cr * dr - ci * di;
+      dli = cr * di + ci * dr;
+      tmp = p * dlr - q * dli;
+      q = p * dli + q * dlr;
+      p = tmp;
+      if (fabs(dlr - T(1)) + fabs(dli) < eps) break;
+    }
+    if (i >= BesselK<T>::MAXIT) note_unconverged();
   }
   const T gam = (p - f) / q;
   T rjmu = bx::sqrt_(w / ((p - f) * gam + q));
@@ -438,20 +459,24 @@ __device__ inline IK<T> besselik_pos(T nu, T x, bool& scaled) {
     T q1 = 0, q2 = 1;
     const T a1 = T(0.25) - mu * mu;
     T q = a1, c = a1, a = -a1, s = T(1) + q * delh;
-    for (int i = 2; i < BesselK<T>::MAXIT; ++i) {
-      a -= T(2 * (i - 1));
-      c = -a * c / T(i);
-      const T qn = (q1 - b * q2) / a;
-      q1 = q2;
-      q2 = qn;
-      q += c * qn;
-      b += T(2);
-      d = T(1) / (b + a * d);
-      delh = (b * d - T(1)) * delh;
-      h += delh;
-      const T dels = q * delh;
-      s += dels;
-      if (fabs(dels / s) < eps) break;
+    {  // counted loop: reaching the cap is recorded (note_unconverged)
+      int i = 2;
+      for (; i < BesselK<T>::MAXIT; ++i) {
+        a -= T(2 * (i - 1));
+        c = -a * c / T(i);
+        const T qn = (q1 - b * q2) / a;
+        q1 = q2;
+        q2 = qn;
+        q += c * qn;
+        b += T(2);
+        d = T(1) / (b + a * d);
+        delh = (b * d - T(1)) * delh;
+        h += delh;
+        const T dels = q * delh;
+        s += dels;
+        if (fabs(dels / s) < eps) break;
+      }
+      if (i >= BesselK<T>::MAXIT) note_unconverged();
     }
     h = a1 * h;
     k0 = bx::sqrt_(pi / (T(2) * x)) / s;
@@ -478,13 +503,17 @@ __device__ inline IK<T> besselik_pos(T nu, T x, bool& scaled) {
       T h = nu * xi;
       if (h < fpmin) h = fpmin;
       T b = xi2 * nu, d = 0, c = h;
-      for (int i = 1; i < BesselK<T>::MAXIT; ++i) {
-        b += xi2;
-        d = T(1) / (b + d);
-        c = b + T(1) / c;
-        const T del = c * d;
-        h *= del;
-        if (fabs(del - T(1)) < eps) break;
+      {  // counted loop: reaching the cap is recorded (note_unconverged)
+        int i = 1;
+        for (; i < BesselK<T>::MAXIT; ++i) {
+          b += xi2;
+          d = T(1) / (b + d);
+          c = b + T(1) / c;
+          const T del = c * d;
+          h *= del;
+          if (fabs(del - T(1)) < eps) break;
+        }
+        if (i >= BesselK<T>::MAXIT) note_unconverged();
       }
       T ril = fpmin, ripl = h * ril;
       T ril1 = ril, rip1 = ripl, fact = nu * xi;

@@ -30,6 +30,7 @@
 // analytic first derivatives with step ε^(1/3)·a (or ·b).
 #pragma once
 
+#include "unconverged.cuh"
 #include <math_constants.h>
 
 #include "beta_math.cuh"
@@ -79,30 +80,34 @@ __device__ inline IbetaCF ibeta_cf(double p, double q, double y, double sp, doub
     A1 *= s, A2 *= s, B1 *= s, B2 *= s;
     if (DERIVS) Ap1 *= s, Ap2 *= s, Bp1 *= s, Bp2 *= s, Aq1 *= s, Aq2 *= s, Bq1 *= s, Bq2 *= s;
   };
-  for (int m = 0; m < ib::kMaxPairs; ++m) {
-    const double md = m;
-    {  // d_(2m+1)
-      const double u = p + md, v = pq + md, w = p + 2.0 * md, w1 = w + 1.0;
-      const double d = -(u * v * y) / (w * w1);
-      const double dp = d * ((1.0 / u + 1.0 / v) - (1.0 / w + 1.0 / w1));
-      step(d, DERIVS ? dp : 0.0, DERIVS ? d / v : 0.0);
+  {  // counted loop: reaching the cap is recorded (note_unconverged)
+    int m = 0;
+    for (; m < ib::kMaxPairs; ++m) {
+      const double md = m;
+      {  // d_(2m+1)
+        const double u = p + md, v = pq + md, w = p + 2.0 * md, w1 = w + 1.0;
+        const double d = -(u * v * y) / (w * w1);
+        const double dp = d * ((1.0 / u + 1.0 / v) - (1.0 / w + 1.0 / w1));
+        step(d, DERIVS ? dp : 0.0, DERIVS ? d / v : 0.0);
+      }
+      {  // d_(2m+2)
+        const double k = md + 1.0, w = p + 2.0 * md + 1.0, w1 = w + 1.0;
+        const double r = k * y / (w * w1);
+        const double d = (q - k) * r;
+        step(d, DERIVS ? -d * (1.0 / w + 1.0 / w1) : 0.0, r);
+      }
+      const double Kn = A1 / B1;
+      bool done = fabs(Kn - K) <= ib::kTol * fabs(Kn);
+      if (DERIVS) {
+        const double Kpn = (Ap1 - Kn * Bp1) / B1, Kqn = (Aq1 - Kn * Bq1) / B1;
+        done = done && fabs(Kpn - Kp) <= ib::kTolD * (fabs(Kpn) + fabs(Kn) * sp) &&
+               fabs(Kqn - Kq) <= ib::kTolD * (fabs(Kqn) + fabs(Kn) * sq);
+        Kp = Kpn, Kq = Kqn;
+      }
+      K = Kn;
+      if (done) break;
     }
-    {  // d_(2m+2)
-      const double k = md + 1.0, w = p + 2.0 * md + 1.0, w1 = w + 1.0;
-      const double r = k * y / (w * w1);
-      const double d = (q - k) * r;
-      step(d, DERIVS ? -d * (1.0 / w + 1.0 / w1) : 0.0, r);
-    }
-    const double Kn = A1 / B1;
-    bool done = fabs(Kn - K) <= ib::kTol * fabs(Kn);
-    if (DERIVS) {
-      const double Kpn = (Ap1 - Kn * Bp1) / B1, Kqn = (Aq1 - Kn * Bq1) / B1;
-      done = done && fabs(Kpn - Kp) <= ib::kTolD * (fabs(Kpn) + fabs(Kn) * sp) &&
-             fabs(Kqn - Kq) <= ib::kTolD * (fabs(Kqn) + fabs(Kn) * sq);
-      Kp = Kpn, Kq = Kqn;
-    }
-    K = Kn;
-    if (done) break;
+    if (m >= ib::kMaxPairs) note_unconverged();
   }
   return {K, Kp, Kq};
 }

@@ -37,6 +37,7 @@
 #include <type_traits>
 
 #include "torchscience_b200.h"
+#include "unconverged.cuh"
 
 namespace tsb {
 
