@@ -891,8 +891,6 @@ def secondary_arm(args):
         ref_cpu = None
         if not args.no_cpu_baseline:
             try:
-                import time
-
                 import numpy as np
 
                 from oracle import oracle as O
@@ -916,7 +914,7 @@ def secondary_arm(args):
 
             row["fwd_bwd_gelem_s"] = _rate(fb, n, S, W, flush)
             if ref_cpu is not None:
-                O, np, time = ref_cpu
+                O, np, _ = ref_cpu
                 m = 1 << 14
                 sample = [t[:m].cpu().numpy() for t in ins]
                 key = {"chi2_cumulative_distribution": "chi2_cumulative_distribution",

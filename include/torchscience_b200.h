@@ -53,7 +53,9 @@ typedef enum tsb_dtype {
   TSB_F32 = 0,
   TSB_F64 = 1,
   TSB_F16 = 2,
-  TSB_BF16 = 3
+  TSB_BF16 = 3,
+  TSB_C64 = 4,   /* complex64: interleaved float real, imaginary */
+  TSB_C128 = 5   /* complex128: interleaved double real, imaginary */
 } tsb_dtype;
 
 typedef enum tsb_precision {

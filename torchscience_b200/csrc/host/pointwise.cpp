@@ -19,8 +19,22 @@ int32_t to_tsb_dtype(at::ScalarType t) {
     case at::kDouble: return TSB_F64;
     case at::kHalf: return TSB_F16;
     case at::kBFloat16: return TSB_BF16;
+    case at::kComplexFloat: return TSB_C64;
+    case at::kComplexDouble: return TSB_C128;
     default: TORCH_CHECK(false, "torchscience_b200: unsupported dtype ", t);
   }
+}
+
+// Operators with complex64 / complex128 kernels (and their backward and
+// double-backward ops).
+bool takes_complex(const char* name) {
+  static const char* const ops[] = {"log_gamma", "gamma", "digamma", "trigamma"};
+  const std::string n(name);
+  for (const char* op : ops) {
+    const std::string o(op);
+    if (n == o || n == o + "_backward" || n == o + "_backward_backward") return true;
+  }
+  return false;
 }
 
 // Descriptor of `t` viewed over the iteration shape `shape` (t must be
@@ -71,8 +85,13 @@ at::ScalarType checked_common_dtype(const char* name, at::TensorList inputs) {
   at::native::ResultTypeState state = {};
   for (const auto& t : inputs) state = at::native::update_result_type_state(t, state);
   const at::ScalarType dt = at::native::result_type(state);
-  TORCH_CHECK_NOT_IMPLEMENTED(!at::isComplexType(dt), "\"", name, "\" not implemented for '", c10::toString(dt),
-                              "' in torchscience_b200 (real dtypes only)");
+  if (at::isComplexType(dt)) {
+    TORCH_CHECK_NOT_IMPLEMENTED(takes_complex(name), "\"", name, "\" not implemented for '", c10::toString(dt),
+                                "' in torchscience_b200 (complex dtypes: log_gamma, gamma, digamma, trigamma)");
+    TORCH_CHECK_NOT_IMPLEMENTED(dt == at::kComplexFloat || dt == at::kComplexDouble, "\"", name,
+                                "\" not implemented for '", c10::toString(dt), "'");
+    return dt;
+  }
   TORCH_CHECK_NOT_IMPLEMENTED(at::isFloatingType(dt), "\"", name, "\" not implemented for '", c10::toString(dt), "'");
   TORCH_CHECK_NOT_IMPLEMENTED(dt == at::kFloat || dt == at::kDouble || dt == at::kHalf || dt == at::kBFloat16, "\"",
                               name, "\" not implemented for '", c10::toString(dt), "'");

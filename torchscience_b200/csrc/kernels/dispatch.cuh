@@ -44,6 +44,8 @@ inline int32_t dtype_size(int32_t dt) {
     case TSB_F64: return 8;
     case TSB_F16: return 2;
     case TSB_BF16: return 2;
+    case TSB_C64: return 8;
+    case TSB_C128: return 16;
     default: return 0;
   }
 }
@@ -342,6 +344,8 @@ int32_t run_op(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_
   if (st) return st;
   if (precision != TSB_PRECISION_AUTO && precision != TSB_PRECISION_FP64)
     return set_error(TSB_ERR_ARGUMENT, "unknown precision mode %d", precision);
+  if (dtype == TSB_C64 || dtype == TSB_C128)
+    return set_error(TSB_ERR_DTYPE, "this entry point takes real dtypes only");
   uint32_t mask = 0;
   for (int o = 0; o < NOUT; ++o)
     if (out[o].data) mask |= 1u << o;
@@ -419,10 +423,52 @@ int32_t run_op(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_
   }
 }
 
+// Entry point body for complex64 / complex128 data: the map kernel over a
+// complex128 functor, no reduced outputs.
+template <class CF>
+int32_t run_complex(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_t n_out, int32_t precision,
+                    void* stream_ptr) {
+  constexpr int NIN = CF::NIN, NOUT = CF::NOUT;
+  Canon c;
+  int32_t dtype = 0;
+  int32_t st = canonicalize(in, n_in, out, n_out, NIN, NOUT, c, dtype);
+  if (st) return st;
+  if (precision != TSB_PRECISION_AUTO && precision != TSB_PRECISION_FP64)
+    return set_error(TSB_ERR_ARGUMENT, "unknown precision mode %d", precision);
+  uint32_t mask = 0;
+  for (int o = 0; o < NOUT; ++o)
+    if (out[o].data) mask |= 1u << o;
+  if (c.numel == 0 || mask == 0) return TSB_OK;
+  for (int o = 0; o < NOUT; ++o)
+    if ((mask & (1u << o)) && output_is_reduced(c, NIN + o))
+      return set_error(TSB_ERR_LAYOUT, "complex entry points do not reduce outputs");
+  int dev = 0;
+  const DeviceInfo* info = nullptr;
+  st = current_device(&dev, &info);
+  if (st) return st;
+  MapParams<NIN, NOUT> p;
+  fill_map_params(c, in, out, mask, p);
+  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
+  switch (dtype) {
+    case TSB_C64: return launch_map<CF, cuda::std::complex<float>>(p, s, dev, info);
+    case TSB_C128: return launch_map<CF, cuda::std::complex<double>>(p, s, dev, info);
+  }
+  return set_error(TSB_ERR_DTYPE, "unsupported dtype");
+}
+
 }  // namespace tsb
 
 // Defines one C-ABI entry point that forwards to run_op<Functor>.
 #define TSB_DEFINE_OP(cname, Functor)                                                                  \
   extern "C" TSB_OP_SIGNATURE(cname) {                                                                 \
     return tsb::run_op<Functor>(in, n_in, out, n_out, precision, workspace, workspace_bytes, stream); \
+  }
+
+// An entry point that also takes complex64 / complex128 data (run_complex
+// with CFunctor, a complex128 functor).
+#define TSB_DEFINE_OP_C(cname, Functor, CFunctor)                                                         \
+  extern "C" TSB_OP_SIGNATURE(cname) {                                                                   \
+    if (n_in > 0 && in && (in[0].dtype == TSB_C64 || in[0].dtype == TSB_C128))                           \
+      return tsb::run_complex<CFunctor>(in, n_in, out, n_out, precision, stream);                        \
+    return tsb::run_op<Functor>(in, n_in, out, n_out, precision, workspace, workspace_bytes, stream);   \
   }

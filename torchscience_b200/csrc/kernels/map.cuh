@@ -34,6 +34,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cuda/std/complex>
+
 #include <type_traits>
 
 #include "torchscience_b200.h"
@@ -109,6 +111,30 @@ __device__ __forceinline__ void store_as<__half, double>(char* p, double v) {
 template <>
 __device__ __forceinline__ void store_as<__nv_bfloat16, double>(char* p, double v) {
   *reinterpret_cast<__nv_bfloat16*>(p) = __double2bfloat16(v);
+}
+
+// Complex storage (interleaved real, imaginary) with complex128 arithmetic.
+template <>
+__device__ __forceinline__ cuda::std::complex<double> load_as<cuda::std::complex<float>, cuda::std::complex<double>>(
+    const char* p) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  return cuda::std::complex<double>(v.x, v.y);
+}
+template <>
+__device__ __forceinline__ cuda::std::complex<double> load_as<cuda::std::complex<double>, cuda::std::complex<double>>(
+    const char* p) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  return cuda::std::complex<double>(v.x, v.y);
+}
+template <>
+__device__ __forceinline__ void store_as<cuda::std::complex<float>, cuda::std::complex<double>>(
+    char* p, cuda::std::complex<double> v) {
+  *reinterpret_cast<float2*>(p) = make_float2((float)v.real(), (float)v.imag());
+}
+template <>
+__device__ __forceinline__ void store_as<cuda::std::complex<double>, cuda::std::complex<double>>(
+    char* p, cuda::std::complex<double> v) {
+  *reinterpret_cast<double2*>(p) = make_double2(v.real(), v.imag());
 }
 
 // Element offsets of linear index i for every operand (row-major iteration).
