@@ -82,8 +82,8 @@ def test_workspace_query_for_the_broadcast_grid():
     n = L.tsb_workspace_bytes(arr(g, a, x), 3, arr(ga, gx), 2)
     # row-reduced: 128 column tiles x 4096 rows; column-reduced: 128 row tiles (32 rows) x 4096 cols (doubles);
     # then the row-sorted sweep's scratch: the row order (4096 int32), row and column tables (16 doubles per
-    # row and per column) and the task counter (256 bytes)
-    sweep = 4096 * 4 + (4096 + 4096) * 16 * 8 + 256
+    # row and per column), one 32-bit column mask per task of 32 x 32 elements, and the task counters (256 bytes)
+    sweep = 4096 * 4 + (4096 + 4096) * 16 * 8 + 128 * 128 * 4 + 256
     assert n == (128 + 128) * 4096 * 8 + sweep
     # no reduced output: only the sweep's scratch on an (R, 1) x (1, C) grid
     assert L.tsb_workspace_bytes(arr(g, a, x), 3, arr(desc(shape), desc(shape)), 2) == sweep

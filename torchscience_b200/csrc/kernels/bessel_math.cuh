@@ -244,6 +244,17 @@ __device__ inline void recur_up(T mu, T x, int n, T s, T& c0, T& c1) {
   }
 }
 
+// recur_up with the recurrence carried in FP64 for both flavours (for
+// double data it is recur_up itself): a few FP64 operations per step with no
+// division, where FP32 would add ~1e-6 over ~20 steps.
+template <typename T>
+__device__ __forceinline__ void recur_up_fp64(T mu, T x, int n, T s, T& c0, T& c1) {
+  double d0 = c0, d1 = c1;
+  recur_up<double>((double)mu, (double)x, n, (double)s, d0, d1);
+  c0 = (T)d0;
+  c1 = (T)d1;
+}
+
 // Hankel's asymptotic sums for x >= 25 (DLMF 10.17.3, 10.40.1-2):
 //   P = Σ (-1)^k a_2k / x^2k,  Q = Σ (-1)^k a_2k+1 / x^2k+1,  S± = Σ (±1)^k a_k / x^k,
 // a_k(ν) = Π_{j<=k} (4ν² - (2j-1)²) / (k! 8^k).  Stops at convergence or when
@@ -315,11 +326,11 @@ __device__ inline JY<T> besseljy_pos(T nu, T x) {
       c[o][1] = amp * (P * sw + Q * cw);
     }
     T j0 = c[0][0], j1 = c[1][0], y0 = c[0][1], y1 = c[1][1];
-    recur_up<T>(mu, x, nl, T(1), j0, j1);
+    recur_up_fp64<T>(mu, x, nl, T(1), j0, j1);
     r.j = j0;
     r.jp = nu / x * j0 - j1;
     if (NEED_Y) {
-      recur_up<T>(mu, x, nl, T(1), y0, y1);
+      recur_up_fp64<T>(mu, x, nl, T(1), y0, y1);
       r.y = y0;
       r.yp = nu / x * y0 - y1;
     }
@@ -413,7 +424,7 @@ __device__ inline JY<T> besseljy_pos(T nu, T x) {
   r.jp = rjp1 * fact;
   if (NEED_Y) {
     T y0 = rymu, y1 = ry1;
-    recur_up<T>(mu, x, nl, T(1), y0, y1);
+    recur_up_fp64<T>(mu, x, nl, T(1), y0, y1);
     r.y = y0;
     r.yp = nu * xi * y0 - y1;
   }
@@ -491,13 +502,17 @@ __device__ inline IK<T> besselik_pos(T nu, T x, bool& scaled) {
       T i0 = ai * Sm, i1 = ai * Sm1;
       // I_{k+1} = I_{k-1} - (2k/x) I_k; for x >= ν²/2 the error growth of
       // this (mildly unstable) upward recurrence stays below e².
+      // the recurrence in FP64 for both flavours: a few FP64 operations per
+      // step, where FP32 would add ~1e-6 over ~20 steps
+      double d0 = i0, d1 = i1;
+      const double dxi2 = (double)xi2;
       for (int i = 1; i <= nl; ++i) {
-        const T t = i0 - (mu + T(i)) * xi2 * i1;
-        i0 = i1;
-        i1 = t;
+        const double t = d0 - ((double)mu + (double)i) * dxi2 * d1;
+        d0 = d1;
+        d1 = t;
       }
-      r.i = i0;
-      r.ip = nu * xi * i0 + i1;
+      r.i = (T)d0;
+      r.ip = (T)((double)(nu * xi) * d0 + d1);
     } else {
       // CF1 for f = I'_ν/I_ν, downward recurrence to μ, Wronskian with K̃.
       T h = nu * xi;
@@ -538,9 +553,10 @@ __device__ inline IK<T> besselik_pos(T nu, T x, bool& scaled) {
     }
   }
   if (NEED_K) {
-    recur_up<T>(mu, x, nl, T(-1), k0, k1);
-    r.k = k0;
-    r.kp = nu * xi * k0 - k1;
+    double d0 = k0, d1 = k1;  // the recurrence in FP64 for both flavours, as for I above
+    recur_up<double>((double)mu, (double)x, nl, -1.0, d0, d1);
+    r.k = (T)d0;
+    r.kp = (T)((double)(nu * xi) * d0 - d1);
   }
   return r;
 }

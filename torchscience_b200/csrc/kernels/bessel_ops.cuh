@@ -178,12 +178,16 @@ __device__ inline BesselNuDerivs bessel_nu_derivs(double nu, double x, const BV<
   return o;
 }
 
-// Value (+ d/dx): FP32 in the mixed kernels' kBsSeries region, FP64 otherwise;
-// non-finite FP32 results (values at the edge of FP32 range) are redone in FP64.
+// Value (+ d/dx) in the mixed kernels: FP32 in the kBsSeries region, and for
+// I and K (which have no zeros, so FP32 keeps its relative accuracy) also in
+// the Steed and Hankel regions, with the order recurrences in FP64; FP64
+// otherwise.  Non-finite FP32 results (values at the edge of FP32 range) are
+// redone in FP64.
 template <typename T, int KIND>
 __device__ __forceinline__ BV<T> bessel_value(int region, T nu, T x) {
   if constexpr (std::is_same<T, float>::value) {
-    if (region == kBsSeries) {
+    const bool fp32 = region == kBsSeries || ((KIND == kBI || KIND == kBK) && (region == kBsMid || region == kBsLarge));
+    if (fp32) {
       const BV<float> f = bessel_eval<float, KIND>(nu, x);
       if (isfinite(f.v) && isfinite(f.d)) return f;
     }
@@ -194,13 +198,58 @@ __device__ __forceinline__ BV<T> bessel_value(int region, T nu, T x) {
   }
 }
 
+// J and Y in the mixed kernels' Steed and Hankel regions: FP32, with the
+// elements next to a zero of the requested quantity declined to the FP64
+// evaluator (the map kernel's rescue list).  Near a zero the FP32 result keeps
+// its absolute accuracy, about 3 ulp of the local modulus M, but not its
+// relative accuracy.  With the Debye phase rate w = sqrt(1 - (ν/x)²) the
+// modulus is M² ≈ C² + (C'/w)²; an FP32 value is kept when |C| >= 0.3 M, a
+// derivative when |C'| >= 0.3 w M, which bounds their relative error by
+// about 3·6e-8 / 0.3 = 6e-7.  For x <= ν neither function has a zero.
+constexpr float kBsKeep = 0.3f;
+__device__ __forceinline__ bool bessel_fp32_kept(float nu, float x, float v, float d, bool deriv) {
+  if (!isfinite(v) || !isfinite(d)) return false;
+  const float r = fabsf(nu) / x;
+  if (r >= 1.0f) return true;
+  const float w2 = 1.0f - r * r;
+  const float m2 = v * v + d * d / w2;
+  if (!isfinite(m2)) return false;
+  return deriv ? d * d >= kBsKeep * kBsKeep * w2 * m2 : v * v >= kBsKeep * kBsKeep * m2;
+}
+template <typename T, int KIND>
+__device__ __forceinline__ bool bessel_first(int region, T nu, T x, bool deriv, BV<T>& out) {
+  if constexpr (std::is_same<T, float>::value && (KIND == kBJ || KIND == kBY)) {
+    if ((region == kBsMid || region == kBsLarge) && nu >= 0.0f && x > 0.0f) {
+      const BV<float> f = bessel_eval<float, KIND>(nu, x);
+      if (!bessel_fp32_kept(nu, x, f.v, f.d, deriv)) return false;
+      out = f;
+      return true;
+    }
+  }
+  out = bessel_value<T, KIND>(region, nu, x);
+  return true;
+}
+template <typename T, int KIND>
+__device__ __forceinline__ BV<T> bessel_rescue(T nu, T x) {
+  const BV<double> dd = bessel_eval<double, KIND>((double)nu, (double)x);
+  return {(T)dd.v, (T)dd.d};
+}
+
 template <int KIND, typename T_>
 struct BesselFwd {
   using T = T_;
   static constexpr int NIN = 2, NOUT = 1, R = kBsRegions;
   static constexpr bool REDUCE = false;
+  static constexpr bool RESCUE = std::is_same<T, float>::value && (KIND == kBJ || KIND == kBY);
   __device__ static int classify(const T* in) { return bessel_classify<KIND>((double)in[0], (double)in[1]); }
   __device__ static void eval(int r, const T* in, T* out, uint32_t) { out[0] = bessel_value<T, KIND>(r, in[0], in[1]).v; }
+  __device__ static bool eval_first(int r, const T* in, T* out, uint32_t) {
+    BV<T> b;
+    if (!bessel_first<T, KIND>(r, in[0], in[1], false, b)) return false;
+    out[0] = b.v;
+    return true;
+  }
+  __device__ static void eval_rescue(int, const T* in, T* out, uint32_t) { out[0] = bessel_rescue<T, KIND>(in[0], in[1]).v; }
 };
 
 // in = {grad, n, z}, out = {grad_n, grad_z}
@@ -221,6 +270,22 @@ struct BesselBwd {
     }
     out[0] = T(0);
     out[1] = in[0] * bessel_value<T, KIND>(r, in[1], in[2]).d;
+  }
+  static constexpr bool RESCUE = std::is_same<T, float>::value && (KIND == kBJ || KIND == kBY);
+  __device__ static bool eval_first(int r, const T* in, T* out, uint32_t mask) {
+    if (mask & 1u) {
+      eval(r, in, out, mask);
+      return true;
+    }
+    BV<T> b;
+    if (!bessel_first<T, KIND>(r, in[1], in[2], true, b)) return false;
+    out[0] = T(0);
+    out[1] = in[0] * b.d;
+    return true;
+  }
+  __device__ static void eval_rescue(int, const T* in, T* out, uint32_t) {
+    out[0] = T(0);
+    out[1] = in[0] * bessel_rescue<T, KIND>(in[1], in[2]).d;
   }
 };
 
@@ -353,11 +418,21 @@ __device__ inline BesselIntVals bessel_int_vals(double z, bool need_d2) {
   return {b.v, b.d, d2};
 }
 
+// Region of an integer-order element (the evaluator's method for z, as in
+// bessel_classify), so that the map kernel groups each warp's lanes by method:
+// the real-order evaluator runs a series, Steed's fractions or Hankel's sums
+// depending on z, and a warp holding all three runs all three.
+template <int KIND, int ORDER>
+__device__ __forceinline__ int bessel_int_classify(double z) {
+  return bessel_classify<KIND>((double)ORDER, z);
+}
+
 template <int KIND, int ORDER, typename T_>
 struct BesselIntFwd {
   using T = T_;
-  static constexpr int NIN = 1, NOUT = 1, R = 1;
+  static constexpr int NIN = 1, NOUT = 1, R = kBsRegions;
   static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return bessel_int_classify<KIND, ORDER>((double)in[0]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     out[0] = (T)bessel_int_vals<KIND, ORDER>((double)in[0], false).v;
   }
@@ -365,8 +440,9 @@ struct BesselIntFwd {
 template <int KIND, int ORDER, typename T_>
 struct BesselIntBwd {  // in = {grad, z}
   using T = T_;
-  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr int NIN = 2, NOUT = 1, R = kBsRegions;
   static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return bessel_int_classify<KIND, ORDER>((double)in[1]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     out[0] = (T)((double)in[0] * bessel_int_vals<KIND, ORDER>((double)in[1], false).d);
   }
@@ -374,8 +450,9 @@ struct BesselIntBwd {  // in = {grad, z}
 template <int KIND, int ORDER, typename T_>
 struct BesselIntBwdBwd {  // in = {gg, grad, z}: {gg·f'(z), gg·grad·f''(z)}
   using T = T_;
-  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr int NIN = 3, NOUT = 2, R = kBsRegions;
   static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return bessel_int_classify<KIND, ORDER>((double)in[2]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     const double gg = in[0], g = in[1];
     const BesselIntVals f = bessel_int_vals<KIND, ORDER>((double)in[2], true);

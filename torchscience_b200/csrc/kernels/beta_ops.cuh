@@ -90,11 +90,26 @@ struct BetaBwdBwd {  // âˆ‚Â²B = B (âˆ‚ ln B âˆ‚ ln B + âˆ‚Â² ln B)
   }
 };
 
+// Region of an order: n = 0 .. 3 take their own evaluators (regions 0 .. 3),
+// higher orders the Hurwitz zeta, whose direct-term count grows with n
+// (buckets of 4 orders up to n = 43, then one more); z < 0 adds the
+// reflection's second sum (its own bucket).  Regions are numbered by
+// decreasing cost.
+constexpr int kPgRegions = 16;
+__device__ __forceinline__ int polygamma_classify(int n, double z) {
+  if (n < 0 || isnan(z)) return kPgRegions - 1;
+  if (z < 0.0) return 0;
+  if (n <= 3) return kPgRegions - 2 - n;  // 14 .. 11
+  const int b = (n - 4) >> 2;               // 0 .. 9 for n < 44
+  return b >= 9 ? 1 : 10 - b;               // 10 .. 2, and 1 for n >= 40
+}
+
 template <typename T_>
 struct PolygammaFwd {  // in = {n, z}
   using T = T_;
-  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr int NIN = 2, NOUT = 1, R = kPgRegions;
   static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return polygamma_classify(polygamma_order(in[0]), in[1]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     out[0] = (T)polygamma_d(polygamma_order(in[0]), in[1]);
   }
@@ -103,8 +118,11 @@ struct PolygammaFwd {  // in = {n, z}
 template <typename T_>
 struct PolygammaBwd {  // in = {grad, n, z}, out = {grad_n = 0, grad_z = gradÂ·Ïˆ^(n+1)(z)}
   using T = T_;
-  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr int NIN = 3, NOUT = 2, R = kPgRegions;
   static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) {
+    return polygamma_classify(polygamma_order((double)in[1] + 1.0), in[2]);
+  }
   __device__ static void eval(int, const T* in, T* out, uint32_t mask) {
     out[0] = T(0);
     out[1] = (mask & 2u) ? (T)((double)in[0] * polygamma_d(polygamma_order((double)in[1] + 1.0), in[2])) : T(0);
@@ -114,8 +132,11 @@ struct PolygammaBwd {  // in = {grad, n, z}, out = {grad_n = 0, grad_z = gradÂ·Ï
 template <typename T_>
 struct PolygammaBwdBwd {  // in = {gg_n, gg_z, grad, n, z}
   using T = T_;
-  static constexpr int NIN = 5, NOUT = 3, R = 1;
+  static constexpr int NIN = 5, NOUT = 3, R = kPgRegions;
   static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) {
+    return polygamma_classify(polygamma_order((double)in[3] + 2.0), in[4]);
+  }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     const double ggz = in[1], g = in[2], n = in[3], z = in[4];
     out[0] = (T)(ggz * polygamma_d(polygamma_order(n + 1.0), z));

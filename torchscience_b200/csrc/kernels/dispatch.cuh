@@ -219,16 +219,15 @@ int32_t launch_reduce(const Canon& c, const tsb_tensor* in, const tsb_tensor* ou
     if (!(p.out_mask & (1u << o))) continue;
     const int kind = p.out_kind[o];
     if (kind == kOutRow) {
-      const unsigned g = (unsigned)((p.rows + kBlock - 1) / kBlock);
-      finalize_kernel<TS><<<g, kBlock, 0, stream>>>(p.ws[o], p.rows, p.n_col_tiles, p.rows, p.out_ptr[o], p.out_s0[o]);
+      launch_finalize<TS>(p.ws[o], p.rows, p.n_col_tiles, p.rows, p.out_ptr[o], p.out_s0[o], stream);
     } else if (kind == kOutCol) {
-      const unsigned g = (unsigned)((p.cols + kBlock - 1) / kBlock);
-      finalize_kernel<TS><<<g, kBlock, 0, stream>>>(p.ws[o], p.cols, p.n_row_tiles, p.cols, p.out_ptr[o], p.out_s1[o]);
+      launch_finalize<TS>(p.ws[o], p.cols, p.n_row_tiles, p.cols, p.out_ptr[o], p.out_s1[o], stream);
     } else if (kind == kOutAll) {
       finalize_all_kernel<TS><<<1, kBlock, 0, stream>>>(p.ws[o], ntiles, p.out_ptr[o]);
+      count_launches(1);
+    } else {
+      continue;
     }
-    if (kind != kOutRow && kind != kOutCol && kind != kOutAll) continue;
-    count_launches(1);
     st = check_launch("finalize kernel launch");
     if (st) return st;
   }
@@ -246,6 +245,24 @@ inline bool sweep_layout(const Canon& c, int ia, int ix, bool& transpose) {
   else return false;
   return c.size[transpose ? 1 : 0] <= kSweepMaxRows;
 }
+
+// Functors whose reducing pass may run through the streaming 2-D kernel
+// (stream2d.cuh): `static constexpr bool STREAM2D = true`.
+template <class Fn, class = void>
+struct Stream2DOptIn {
+  static constexpr bool value = false;
+};
+template <class Fn>
+struct Stream2DOptIn<Fn, decltype((void)Fn::STREAM2D, void())> {
+  static constexpr bool value = Fn::STREAM2D;
+};
+
+// Streaming 2-D reduction; defined in stream2d.cuh, which the units of
+// functors with STREAM2D include.  Returns TSB_ERR_LAYOUT without launching
+// when the layout or the workspace does not suit it.
+template <class Fn, typename TS>
+int32_t launch_stream2d(const Canon& c, const tsb_tensor* in, const tsb_tensor* out, uint32_t mask, void* ws,
+                        int64_t ws_bytes, cudaStream_t stream);
 
 // Runs Fn through the row-sorted sweep; defined in sweep.cuh, which the
 // units of functors with SWEEP include.  Returns TSB_ERR_WORKSPACE without
@@ -409,6 +426,16 @@ int32_t run_op(const tsb_tensor* in, int32_t n_in, const tsb_tensor* out, int32_
     return set_error(TSB_ERR_DTYPE, "unsupported dtype");
   }
   if constexpr (FD::REDUCE) {
+    if constexpr (Stream2DOptIn<FD>::value) {
+      int32_t sr = TSB_ERR_LAYOUT;
+      switch (dtype) {
+        case TSB_F64: sr = launch_stream2d<FD, double>(c, in, out, mask, ws, ws_bytes, s); break;
+        case TSB_F32: sr = launch_stream2d<FF, float>(c, in, out, mask, ws, ws_bytes, s); break;
+        case TSB_F16: sr = launch_stream2d<FF, __half>(c, in, out, mask, ws, ws_bytes, s); break;
+        case TSB_BF16: sr = launch_stream2d<FF, __nv_bfloat16>(c, in, out, mask, ws, ws_bytes, s); break;
+      }
+      if (sr != TSB_ERR_LAYOUT) return sr;
+    }
     switch (dtype) {
       case TSB_F64: return launch_reduce<FD, double>(c, in, out, mask, ws, ws_bytes, s, dev, info);
       case TSB_F32:

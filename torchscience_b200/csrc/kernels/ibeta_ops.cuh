@@ -155,11 +155,31 @@ __device__ __forceinline__ bool ibeta_params_ok(double a, double b) {
   return a > 0.0 && b > 0.0 && isfinite(a) && isfinite(b);
 }
 
+// Region of (x, a, b) by the expected length of the continued fraction, so
+// that the map kernel gives each warp lanes of similar cost: the fraction
+// takes longer the larger the smaller parameter (bucketed by its binary
+// logarithm, 0 .. 6) and the closer x lies to the swap point
+// (a+1)/(a+b+2), within three standard deviations of the beta distribution
+// or not.  The closed forms (a = 1 or b = 1) and the points outside the
+// domain are regions of their own.  Numbered by decreasing cost.
+constexpr int kIbRegions = 16;
+__device__ __forceinline__ int ibeta_classify(double xd, double ad, double bd) {
+  if (!(xd > 0.0 && xd < 1.0) || !ibeta_params_ok(ad, bd)) return kIbRegions - 1;
+  if (ad == 1.0 || bd == 1.0) return kIbRegions - 2;
+  const float x = (float)xd, a = (float)ad, b = (float)bd;
+  const int lb = min(6, (int)__log2f(1.0f + fminf(a, b)));
+  const float s = a + b, xs = (a + 1.0f) / (s + 2.0f);
+  const float sd = sqrtf(a * b / (s * s * (s + 1.0f)));
+  const bool near = fabsf(x - xs) < 3.0f * sd;
+  return (6 - lb) * 2 + (near ? 0 : 1);
+}
+
 template <typename T_>
 struct IbetaFwd {  // in = {x, a, b}
   using T = T_;
-  static constexpr int NIN = 3, NOUT = 1, R = 1;
+  static constexpr int NIN = 3, NOUT = 1, R = kIbRegions;
   static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return ibeta_classify(in[0], in[1], in[2]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     const double x = in[0], a = in[1], b = in[2];
     double v;
@@ -178,8 +198,9 @@ struct IbetaFwd {  // in = {x, a, b}
 template <typename T_>
 struct IbetaBwd {  // in = {grad, x, a, b}, out = {grad_x, grad_a, grad_b}
   using T = T_;
-  static constexpr int NIN = 4, NOUT = 3, R = 1;
+  static constexpr int NIN = 4, NOUT = 3, R = kIbRegions;
   static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return ibeta_classify(in[1], in[2], in[3]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t mask) {
     const double g = in[0], x = in[1], a = in[2], b = in[3];
     double gx = 0.0, ga = 0.0, gb = 0.0;
@@ -201,8 +222,9 @@ struct IbetaBwd {  // in = {grad, x, a, b}, out = {grad_x, grad_a, grad_b}
 template <typename T_>
 struct IbetaBwdBwd {  // in = {gg_x, gg_a, gg_b, grad, x, a, b}, out = {grad_grad_output, grad_x, grad_a, grad_b}
   using T = T_;
-  static constexpr int NIN = 7, NOUT = 4, R = 1;
+  static constexpr int NIN = 7, NOUT = 4, R = kIbRegions;
   static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return ibeta_classify(in[4], in[5], in[6]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     const double ggx = in[0], gga = in[1], ggb = in[2], g = in[3], x = in[4], a = in[5], b = in[6];
     if (x <= 0.0 || x >= 1.0) {

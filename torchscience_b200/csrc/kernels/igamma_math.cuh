@@ -340,27 +340,43 @@ struct IgammaOut {
 // iteration count, so the lanes of a warp run loops of similar length.
 enum IgammaRegion : int {
   // Numbered by decreasing cost (measured per element on B200), so that a
-  // tile's sorted list starts with its most expensive groups.  The cheap
-  // regions are split by the ratio that sets their iteration count, so that
-  // the lanes of a warp run loops of similar length.  The mixed forward also
-  // buckets the a < 1 continued fractions, which it runs in FP32 (kIgCa).
-  kIgS3 = 0,         // series, x/(a+1) < 1
-  kIgC2 = 1,         // continued fraction, x/(a+1) <= 1.5
-  kIgC1 = 2,         // continued fraction, x/(a+1) > 1.5
-  kIgS2 = 3,         // series, x/(a+1) < 0.7
-  kIgC0 = 4,         // continued fraction, 3 < x/(a+1) <= 10
-  kIgCa = 5,         // mixed forward only: continued fraction, a < 1 (FP32 there)
-  kIgS1 = 6,         // series, x/(a+1) < 0.35
-  kIgS0 = 7,         // series, 0.01 <= x/(a+1) < 0.1
-  kIgSmallA = 8,     // a < 1, 0.1 (a+1) <= x < a + 1: series for P, dedicated formula for Q
-  kIgC00 = 9,        // continued fraction, x/(a+1) > 10
-  kIgS00 = 10,       // series, x/(a+1) < 0.01
-  kIgSmallA0 = 11,   // a < 1, x < 0.1 (a+1)
-  kIgSat1 = 12,      // Q and every derivative underflow to 0 (P = 1)
-  kIgSat0 = 13,      // P and every derivative underflow to 0 (Q = 1)
-  kIgSpecial = 14,   // NaN / domain / x == 0 / x == inf
-  kIgRegions = 15
+  // tile's sorted list starts with its most expensive groups.  The regions
+  // are split by what sets their iteration count, so that the lanes of a warp
+  // run loops of similar length: the ratio x/(a+1) and, next to the
+  // transition x ~ a, where the term count grows like √a, the size of a
+  // (kIgS3 / kIgC2 for a < 16, then the B, C, D buckets at 16, 64 and 256).
+  // The mixed forward also buckets the a < 1 continued fractions, which it
+  // runs in FP32 (kIgCa).
+  kIgS3D = 0,        // series, x/(a+1) >= 0.7, a >= 256
+  kIgC2D = 1,        // continued fraction, x/(a+1) <= 1.5, a >= 256
+  kIgS3C = 2,        // as kIgS3D, 64 <= a < 256
+  kIgC2C = 3,        // as kIgC2D, 64 <= a < 256
+  kIgS3B = 4,        // as kIgS3D, 16 <= a < 64
+  kIgC2B = 5,        // as kIgC2D, 16 <= a < 64
+  kIgS3 = 6,         // series, 0.7 <= x/(a+1) < 1, a < 16
+  kIgC2 = 7,         // continued fraction, x/(a+1) <= 1.5, a < 16
+  kIgC1 = 8,         // continued fraction, x/(a+1) > 1.5
+  kIgS2 = 9,         // series, x/(a+1) < 0.7
+  kIgC0 = 10,        // continued fraction, 3 < x/(a+1) <= 10
+  kIgCa = 11,        // mixed forward only: continued fraction, a < 1 (FP32 there)
+  kIgS1 = 12,        // series, x/(a+1) < 0.35
+  kIgS0 = 13,        // series, 0.01 <= x/(a+1) < 0.1
+  kIgSmallA = 14,    // a < 1, 0.1 (a+1) <= x < a + 1: series for P, dedicated formula for Q
+  kIgC00 = 15,       // continued fraction, x/(a+1) > 10
+  kIgS00 = 16,       // series, x/(a+1) < 0.01
+  kIgSmallA0 = 17,   // a < 1, x < 0.1 (a+1)
+  kIgSat1 = 18,      // Q and every derivative underflow to 0 (P = 1)
+  kIgSat0 = 19,      // P and every derivative underflow to 0 (Q = 1)
+  kIgSpecial = 20,   // NaN / domain / x == 0 / x == inf
+  kIgRegions = 21
 };
+
+// The transition regions (kIgS3 for the series, kIgC2 for the continued
+// fraction) bucketed by the size of a.
+__device__ __forceinline__ int igamma_transition_bucket(bool cf, float a) {
+  const int base = a >= 256.0f ? kIgS3D : a >= 64.0f ? kIgS3C : a >= 16.0f ? kIgS3B : kIgS3;
+  return base + (cf ? 1 : 0);
+}
 
 // Regions whose loops are short enough for FP32 accumulation (mixed kernels).
 __device__ __forceinline__ bool igamma_fp32_ok(int region) {
@@ -390,12 +406,13 @@ __device__ __forceinline__ int igamma_classify(double ad, double xd, const IgPre
     // P <= D·(a+1)/(a+1-x) ~ D·a.
     if (can_saturate && lnd + P.la1f() + lratio < -760.0f) return kIgSat0;
     if (a < 1.0f) return lam < 0.1f ? kIgSmallA0 : kIgSmallA;
-    return lam < 0.01f ? kIgS00 : lam < 0.1f ? kIgS0 : lam < 0.35f ? kIgS1 : lam < 0.7f ? kIgS2 : kIgS3;
+    return lam < 0.01f ? kIgS00 : lam < 0.1f ? kIgS0 : lam < 0.35f ? kIgS1 : lam < 0.7f ? kIgS2
+                                                                                : igamma_transition_bucket(false, a);
   }
   // Q = a D F with F <= 1/(x+1-a) <= 1.
   if (can_saturate && lnd + P.laf() + lratio < -760.0f) return kIgSat1;
   if (mixed_fwd && a < 1.0f) return kIgCa;
-  return lam > 10.0f ? kIgC00 : lam > 3.0f ? kIgC0 : lam > 1.5f ? kIgC1 : kIgC2;
+  return lam > 10.0f ? kIgC00 : lam > 3.0f ? kIgC0 : lam > 1.5f ? kIgC1 : igamma_transition_bucket(true, a);
 }
 __device__ __forceinline__ int igamma_classify(double ad, double xd, bool mixed_fwd = false) {
   return igamma_classify(ad, xd, IgPre{nullptr, nullptr, ad, xd}, mixed_fwd);
@@ -558,6 +575,16 @@ __device__ __forceinline__ float ff_exp_mul(IgFF v, float m) {
   if (v.hi > -80.0f) return expf(v.hi) * (1.0f + v.lo) * m;
   return (expf(v.hi + 64.0f) * (1.0f + v.lo) * m) * 1.60381089e-28f;
 }
+// The same for several factors of one exponential: exp(v) = m·s, and
+// ff_exp_apply(e, f) = (m·f)·s rounds exactly as ff_exp_mul(v, f) does.
+struct IgFFExp {
+  float m, s;
+};
+__device__ __forceinline__ IgFFExp ff_exp_split(IgFF v) {
+  if (v.hi > -80.0f) return IgFFExp{expf(v.hi) * (1.0f + v.lo), 1.0f};
+  return IgFFExp{expf(v.hi + 64.0f) * (1.0f + v.lo), 1.60381089e-28f};
+}
+__device__ __forceinline__ float ff_exp_apply(IgFFExp e, float f) { return (e.m * f) * e.s; }
 
 // Regions whose first derivatives the mixed kernels evaluate in FP32 (bit r
 // for region r); the others, and every second derivative, run in FP64.
@@ -628,32 +655,38 @@ __device__ inline IgammaOut igamma_eval_mf1(int region, float a, float x, const 
   }
   const IgFF lnE = ff_add(lnD, la);
   const IgFF lnEx = ff_add(lnE, ff_neg(lx));  // ln(E/x) = ln ∂P/∂x
-  o.px = ff_exp_mul(lnEx, 1.0f);
+  // one exponential per distinct exponent: ∂P/∂x shares ln(E/x) with the
+  // expansion's value and a-derivative; the series and the fraction take a
+  // second one, of ln D or ln E
+  const IgFFExp ex = ff_exp_split(lnEx);
+  o.px = ff_exp_apply(ex, 1.0f);
   if (region == kIgC0 || region == kIgC00) {
     // Q = (E/x) S, ∂Q/∂a = (E/x) (E1 S + S1), E1 = ln x - ψ(a) (x >= 20 here)
     float S, S1;
     const IgFF E1 = ff_add(lx, ff_neg(P.psff()));
     igamma_asym_f(a, x, fabsf(E1.hi), S, S1);
-    const float qv = ff_exp_mul(lnEx, S);
+    const float qv = ff_exp_apply(ex, S);
     o.q = qv;
     o.p = 1.0 - (double)qv;
-    o.pa = -(double)ff_exp_mul(lnEx, fmaf(E1.hi, S, fmaf(E1.lo, S, S1)));
+    o.pa = -(double)ff_exp_apply(ex, fmaf(E1.hi, S, fmaf(E1.lo, S, S1)));
   } else if (region != kIgC1 && region != kIgC2) {
     float S, S1, S2;
     igamma_series<float, 1>(a, x, S, S1, S2);
     const IgFF L1 = ff_add(lx, ff_neg(P.prff()));
-    const float pv = ff_exp_mul(lnD, S);
+    const IgFFExp ed = ff_exp_split(lnD);
+    const float pv = ff_exp_apply(ed, S);
     o.p = pv;
     o.q = 1.0 - (double)pv;
-    o.pa = ff_exp_mul(lnD, fmaf(L1.hi, S, fmaf(L1.lo, S, S1)));
+    o.pa = ff_exp_apply(ed, fmaf(L1.hi, S, fmaf(L1.lo, S, S1)));
   } else {
     float F, F1, F2;
     igamma_cf<float, 1>(a, x, F, F1, F2);
     const IgFF E1 = ff_add(lx, ff_neg(P.psff()));
-    const float qv = ff_exp_mul(lnE, F);
+    const IgFFExp ee = ff_exp_split(lnE);
+    const float qv = ff_exp_apply(ee, F);
     o.q = qv;
     o.p = 1.0 - (double)qv;
-    o.pa = -(double)ff_exp_mul(lnE, fmaf(E1.hi, F, fmaf(E1.lo, F, F1)));
+    o.pa = -(double)ff_exp_apply(ee, fmaf(E1.hi, F, fmaf(E1.lo, F, F1)));
   }
   return o;
 }

@@ -7,6 +7,7 @@
 
 #include "dispatch.cuh"
 #include "igamma_math.cuh"
+#include "stream2d.cuh"
 #include "sweep.cuh"
 
 // Resident CTAs the forward's register allocation must allow (64 registers).
@@ -84,9 +85,10 @@ struct IgammaBwd : IgammaAuxIO<1, 1, 2, T_> {
   }
   // Two-pass sweep of float data: pass 1 the FP32 elements, pass 2 the rest.
   static constexpr bool SPLIT = sizeof(T) == 4;
+  // Saturated elements (every derivative 0) take the first pass.
   __device__ static bool fp64_pass(int r, const T* in, uint32_t mask, const double* A, const double* X) {
-    return !(mask & 1u) || r == kIgSat0 || r == kIgSat1 ||
-           igamma_needs_fp64_1(r, (float)in[2], IgammaBwd::pre(in, A, X), false);
+    return !(mask & 1u) || (r != kIgSat0 && r != kIgSat1 &&
+                            igamma_needs_fp64_1(r, (float)in[2], IgammaBwd::pre(in, A, X), false));
   }
   template <int PASS>
   __device__ static void eval_pass(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
@@ -94,7 +96,8 @@ struct IgammaBwd : IgammaAuxIO<1, 1, 2, T_> {
     const double g = in[0];
     const IgPre P = IgammaBwd::pre(in, A, X);
     if constexpr (PASS == 1) {
-      const IgammaOut o = igamma_eval_mf1<false>(r, (float)in[1], (float)in[2], P);
+      const IgammaOut o = (r == kIgSat0 || r == kIgSat1) ? igamma_saturated(r == kIgSat1)
+                                                         : igamma_eval_mf1<false>(r, (float)in[1], (float)in[2], P);
       out[0] = (T)(sgn * g * o.pa);
       out[1] = (T)(sgn * g * o.px);
     } else {
@@ -166,9 +169,11 @@ struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
   // Two-pass sweep of float data: pass 1 the FP32 elements (compact FP32
   // code alone in its kernel), pass 2 the rest in FP64.
   static constexpr bool SPLIT = sizeof(T) == 4;
+  // Saturated elements (P or Q exactly 0 or 1, every derivative 0) take the
+  // first pass.
   __device__ static bool fp64_pass(int r, const T* in, uint32_t mask, const double* A, const double* X) {
-    return !(mask & 2u) || r == kIgSat0 || r == kIgSat1 ||
-           igamma_needs_fp64_1(r, (float)in[1], IgammaFwdGrad::pre(in, A, X), UPPER);
+    return !(mask & 2u) || (r != kIgSat0 && r != kIgSat1 &&
+                            igamma_needs_fp64_1(r, (float)in[1], IgammaFwdGrad::pre(in, A, X), UPPER));
   }
   template <int PASS>
   __device__ static void eval_pass(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
@@ -176,7 +181,8 @@ struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
     const IgPre P = IgammaFwdGrad::pre(in, A, X);
     IgammaOut o;
     if constexpr (PASS == 1) {
-      o = igamma_eval_mf1<UPPER>(r, (float)in[0], (float)in[1], P);
+      o = (r == kIgSat0 || r == kIgSat1) ? igamma_saturated(r == kIgSat1)
+                                         : igamma_eval_mf1<UPPER>(r, (float)in[0], (float)in[1], P);
     } else {
       if (!(mask & 2u)) {
         o = igamma_eval<0, UPPER>(r, (double)in[0], (double)in[1], P);
@@ -204,6 +210,7 @@ struct GradProduct {
   using T = T_;
   static constexpr int NIN = 3, NOUT = 2, R = 1;
   static constexpr bool REDUCE = true;
+  static constexpr bool STREAM2D = true;  // HBM-bound: the streaming 2-D reduction when the layout allows
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     out[0] = in[0] * in[1];
     out[1] = in[0] * in[2];

@@ -334,6 +334,25 @@ __device__ __forceinline__ int cta_sort_by_region(const int (&reg)[EPT], uint16_
   return s_base[R];
 }
 
+// Functors whose fast evaluation may decline an element (RESCUE = true):
+//   __device__ static bool eval_first(int region, const T* in, T* out, uint32_t mask)
+//     evaluates and returns true, or returns false (out untouched) when the
+//     element needs the accurate path, e.g. an FP32 result next to a zero of
+//     the function, where its relative error would exceed the stated bound;
+//   __device__ static void eval_rescue(int region, const T* in, T* out, uint32_t mask)
+//     the accurate path.
+// The declined elements of a tile are collected in shared memory and
+// evaluated after the tile's groups, by consecutive threads, so that a few
+// declined lanes do not hold a whole warp on the slow path.
+template <class Fn, class = void>
+struct HasRescue {
+  static constexpr bool value = false;
+};
+template <class Fn>
+struct HasRescue<Fn, decltype((void)Fn::RESCUE, void())> {
+  static constexpr bool value = Fn::RESCUE;
+};
+
 // Evaluates the sorted tile in place.  Warps take the 32-slot groups of the
 // sorted list dynamically from a shared counter, in list order: regions are
 // numbered by decreasing cost, so the expensive groups start first and the
@@ -343,28 +362,66 @@ __device__ __forceinline__ void cta_eval_groups(int count, typename Fn::T* buf, 
                                                 const uint8_t* regs, uint32_t mask, int* s_next, const double* aux0,
                                                 int mode0, const double* aux1, int mode1) {
   using T = typename Fn::T;
+  constexpr bool RESC = HasRescue<Fn>::value && !AUX;
+  __shared__ uint16_t s_resc[RESC ? TILE : 1];
+  __shared__ int s_nresc;
   const int lane = threadIdx.x & 31;
   const int ngroups = (count + 31) >> 5;
+  if constexpr (RESC) {
+    if (threadIdx.x == 0) s_nresc = 0;
+    __syncthreads();
+  }
   for (;;) {
     int gidx = 0;
     if (lane == 0) gidx = atomicAdd(s_next, 1);
     gidx = __shfl_sync(0xffffffffu, gidx, 0);
     if (gidx >= ngroups) break;
     const int j = (gidx << 5) + lane;
+    bool declined = false;
+    int li = 0;
     if (j < count) {
-      const int li = list[j];
+      li = list[j];
       T v[Fn::NIN], o[Fn::NOUT];
 #pragma unroll
       for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * TILE + li];
+      bool done = true;
       if constexpr (AUX)
         Fn::eval(regs[li], v, o, mask, aux_at<Fn::NAUX0>(aux0, mode0, li), aux_at<Fn::NAUX1>(aux1, mode1, li));
+      else if constexpr (RESC)
+        done = Fn::eval_first(regs[li], v, o, mask);
       else
         Fn::eval(regs[li], v, o, mask);
+      if (done) {
 #pragma unroll
-      for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
+        for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
+      }
+      declined = !done;
+    }
+    if constexpr (RESC) {
+      // warp-aggregated push of the declined lanes' local indices
+      const unsigned b = __ballot_sync(0xffffffffu, declined);
+      if (b) {
+        int base = 0;
+        if (lane == __ffs(b) - 1) base = atomicAdd(&s_nresc, __popc(b));
+        base = __shfl_sync(0xffffffffu, base, __ffs(b) - 1);
+        if (declined) s_resc[base + __popc(b & ((1u << lane) - 1u))] = (uint16_t)li;
+      }
     }
   }
   __syncthreads();
+  if constexpr (RESC) {
+    const int n = s_nresc;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int li = s_resc[k];
+      T v[Fn::NIN], o[Fn::NOUT];
+#pragma unroll
+      for (int q = 0; q < Fn::NIN; ++q) v[q] = buf[q * TILE + li];
+      Fn::eval_rescue(regs[li], v, o, mask);
+#pragma unroll
+      for (int q = 0; q < Fn::NOUT; ++q) buf[q * TILE + li] = o[q];
+    }
+    __syncthreads();
+  }
 }
 
 template <class Fn, typename TS>
@@ -643,15 +700,42 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<Fn>::value) reduce2d_kernel(
   }
 }
 
-// Adds the per-tile partials of one reduced output in tile order.
+// Adds the partials of one reduced output: output i is the sum over k of
+// ws[k * part_stride + i].  A CTA takes 32 outputs; its 8 warps each add
+// every 8th partial (lane = output, so each load instruction of a warp reads
+// 32 consecutive doubles), and warp 0 adds the 8 group sums in warp order,
+// so the result does not depend on scheduling.
+constexpr int kFinGroups = kBlock / 32;
 template <typename TS>
 __global__ void __launch_bounds__(kBlock) finalize_kernel(const double* ws, int64_t n_out, int64_t n_parts,
                                                           int64_t part_stride, char* out, int64_t out_stride) {
-  const int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n_out) return;
-  double s = 0.0;
-  for (int64_t k = 0; k < n_parts; ++k) s += ws[k * part_stride + i];
-  store_as<TS>(out + i * out_stride * (int64_t)sizeof(TS), s);
+  __shared__ double s[kFinGroups][32];
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int64_t i = (int64_t)blockIdx.x * 32 + lane;
+  double v = 0.0;
+  if (i < n_out) {
+#pragma unroll 4
+    for (int64_t k = g; k < n_parts; k += kFinGroups) v += ws[k * part_stride + i];
+  }
+  s[g][lane] = v;
+  __syncthreads();
+  if (g == 0 && i < n_out) {
+    double t = s[0][lane];
+#pragma unroll
+    for (int w = 1; w < kFinGroups; ++w) t += s[w][lane];
+    store_as<TS>(out + i * out_stride * (int64_t)sizeof(TS), t);
+  }
+}
+
+void count_launches(int64_t n);
+
+// Launches finalize_kernel over n_out outputs (and counts the launch).
+template <typename TS>
+inline void launch_finalize(const double* ws, int64_t n_out, int64_t n_parts, int64_t part_stride, char* out,
+                            int64_t out_stride, cudaStream_t stream) {
+  const unsigned g = (unsigned)((n_out + 31) / 32);
+  finalize_kernel<TS><<<g, kBlock, 0, stream>>>(ws, n_out, n_parts, part_stride, out, out_stride);
+  count_launches(1);
 }
 
 // Deterministic sum of n partials (single CTA, fixed tree) into out[0].

@@ -258,11 +258,22 @@ __device__ inline SphNuDerivs sph_nu_derivs(double n, double z, double f0) {
   return o;
 }
 
+// Region of (n, z): the real-order evaluator's method at order n + 1/2 and
+// |z| (bessel_classify), so that the map kernel groups each warp's lanes by
+// method.
+template <int KIND>
+__device__ __forceinline__ int sph_classify(double n, double z) {
+  if (isnan(n) || isnan(z) || fabs(z) < kSphEps) return kBsSpecial;
+  constexpr int KB = KIND == kSphJ ? kBJ : KIND == kSphY ? kBY : KIND == kSphI ? kBI : kBK;
+  return bessel_classify<KB>(n + 0.5, fabs(z));
+}
+
 template <int KIND, typename T_>
 struct SphFwd {  // in = {n, z}
   using T = T_;
-  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr int NIN = 2, NOUT = 1, R = kBsRegions;
   static constexpr bool REDUCE = false;
+  __device__ static int classify(const T* in) { return sph_classify<KIND>((double)in[0], (double)in[1]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     out[0] = (T)sph_eval<KIND, false>((double)in[0], (double)in[1]).v;
   }
@@ -270,8 +281,9 @@ struct SphFwd {  // in = {n, z}
 template <int KIND, typename T_>
 struct SphBwd {  // in = {grad, n, z}, out = {grad_n, grad_z}
   using T = T_;
-  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr int NIN = 3, NOUT = 2, R = kBsRegions;
   static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return sph_classify<KIND>((double)in[1], (double)in[2]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t mask) {
     const double g = in[0], n = in[1], z = in[2];
     const SphVals f = sph_eval<KIND, false>(n, z);
@@ -282,8 +294,9 @@ struct SphBwd {  // in = {grad, n, z}, out = {grad_n, grad_z}
 template <int KIND, typename T_>
 struct SphBwdBwd {  // in = {gg_n, gg_z, grad, n, z}, out = {grad_grad_output, grad_n, grad_z}
   using T = T_;
-  static constexpr int NIN = 5, NOUT = 3, R = 1;
+  static constexpr int NIN = 5, NOUT = 3, R = kBsRegions;
   static constexpr bool REDUCE = true;
+  __device__ static int classify(const T* in) { return sph_classify<KIND>((double)in[3], (double)in[4]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
     const double ggn = in[0], ggz = in[1], g = in[2], n = in[3], z = in[4];
     const SphVals f = sph_eval<KIND, true>(n, z);

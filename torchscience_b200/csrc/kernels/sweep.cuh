@@ -52,6 +52,7 @@ struct Sweep2DParams {
   double* tab_rows;                   // [NAUX0][rows]: table of the k-th sorted row at [j * rows + k]
   double* tab_cols;                   // [cols][NAUX1]
   int32_t* counter;                   // next task (one counter per pass)
+  uint32_t* colmask;                  // per task: the columns holding elements of a split sweep's second pass
   uint32_t out_mask;
 };
 
@@ -65,44 +66,49 @@ __device__ __forceinline__ unsigned int sweep_key(float v) {
   return (b >> 31) ? ~b : (b | 0x80000000u);
 }
 
-// Set-up of a sweep.  Blocks [0, row_blocks) take one row per thread: its
-// rank among the AUX_IN0 values,
+// Set-up of a sweep.  Blocks [0, row_blocks) take 32 rows each, one per
+// lane: the row's rank among the AUX_IN0 values,
 //   rank(i) = #{j : key_j < key_i} + #{j < i : key_j == key_i}
-// (a stable sort, O(rows) comparisons per thread), perm[rank] = i, and the
-// row's table at sorted position rank.  The remaining blocks take one column
-// per thread and fill its table.  Also zeroes the task counter.
+// (a stable sort), with the comparisons split over the block's warps (warp w
+// counts over the w-th eighth of the keys, which its lanes load 32 at a time
+// and pass round by shuffles), perm[rank] = i, and the row's table at sorted
+// position rank.  The remaining blocks take one column per thread and fill
+// its table.  Also zeroes the task counters.
 template <class Fn, typename TS>
-__global__ void __launch_bounds__(kRankBlock) sweep_setup_kernel(const Sweep2DParams<Fn::NIN, Fn::NOUT> p) {
+__global__ void __launch_bounds__(kBlock) sweep_setup_kernel(const Sweep2DParams<Fn::NIN, Fn::NOUT> p) {
   using T = typename Fn::T;
   using KT = typename KeyT<TS>::T;
-  constexpr int IA = Fn::AUX_IN0, IX = Fn::AUX_IN1, N0 = Fn::NAUX0;
-  const int64_t row_blocks = (p.rows + kRankBlock - 1) / kRankBlock;
+  constexpr int IA = Fn::AUX_IN0, IX = Fn::AUX_IN1, N0 = Fn::NAUX0, W = kBlock / 32;
+  const int64_t row_blocks = (p.rows + 31) / 32;
   if ((int64_t)blockIdx.x >= row_blocks) {
-    const int64_t c = ((int64_t)blockIdx.x - row_blocks) * kRankBlock + threadIdx.x;
+    const int64_t c = ((int64_t)blockIdx.x - row_blocks) * kBlock + threadIdx.x;
     if (c < p.cols)
       Fn::make_aux1(load_as<TS, T>(p.in_ptr[IX] + c * p.in_s1[IX] * (int64_t)sizeof(TS)), p.tab_cols + c * Fn::NAUX1);
     return;
   }
-  __shared__ unsigned int s_keys[kRankBlock];
+  __shared__ int s_part[W][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const char* key_ptr = p.in_ptr[IA];
   const int64_t key_stride = p.in_s0[IA] * (int64_t)sizeof(TS), n = p.rows;
-  const int64_t i = (int64_t)blockIdx.x * kRankBlock + threadIdx.x;
+  const int64_t i = (int64_t)blockIdx.x * 32 + lane;
   const unsigned int ki = i < n ? sweep_key((float)load_as<TS, KT>(key_ptr + i * key_stride)) : 0u;
-  int64_t rank = 0;
-  for (int64_t base = 0; base < n; base += kRankBlock) {
-    __syncthreads();
-    const int64_t j = base + threadIdx.x;
-    s_keys[threadIdx.x] = j < n ? sweep_key((float)load_as<TS, KT>(key_ptr + j * key_stride)) : 0xffffffffu;
-    __syncthreads();
-    const int m = (int)(n - base < kRankBlock ? n - base : kRankBlock);
-    int cnt = 0;
+  const int64_t per = (n + W - 1) / W, lo = warp * per, hi = lo + per < n ? lo + per : n;
+  int cnt = 0;
+  for (int64_t base = lo; base < hi; base += 32) {
+    const int64_t jl = base + lane;
+    const unsigned int kl = jl < hi ? sweep_key((float)load_as<TS, KT>(key_ptr + jl * key_stride)) : 0xffffffffu;
+    const int m = (int)(hi - base < 32 ? hi - base : 32);
     for (int t = 0; t < m; ++t) {
-      const unsigned int kj = s_keys[t];
+      const unsigned int kj = __shfl_sync(0xffffffffu, kl, t);
       cnt += (kj < ki) | ((kj == ki) & (base + t < i));
     }
-    rank += cnt;
   }
-  if (i < n) {
+  s_part[warp][lane] = cnt;
+  __syncthreads();
+  if (warp == 0 && i < n) {
+    int64_t rank = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) rank += s_part[w][lane];
     p.perm[rank] = (int32_t)i;
     double tab[N0];
     Fn::make_aux0(load_as<TS, T>(key_ptr + i * key_stride), tab);
@@ -173,51 +179,62 @@ __global__ void __launch_bounds__(kBlock, PASS == 1 ? 4 : SweepMinBlocks<Fn>::va
     const int ncols = (int)(p.cols - c0 < kSweepCols ? p.cols - c0 : kSweepCols);
 #pragma unroll
     for (int q = 0; q < NOUT; ++q) acc[q * 32] = 0.0;
+    // The first pass of a split sweep records which of the task's columns
+    // hold second-pass elements; the second pass visits only those.
+    uint32_t cmask = 0u;
+    if constexpr (PASS == 2) cmask = p.colmask[task];
 
     for (int jj = 0; jj < ncols; ++jj) {
       const int64_t col = c0 + jj;
-      const T x = load_as<TS, T>(p.in_ptr[IX] + col * p.in_s1[IX] * (int64_t)sizeof(TS));
-      const double* xt = p.tab_cols + col * N1;  // every lane reads the same entry
-      // classify and fp64_pass read only the two table inputs; the others
-      // (e.g. an upstream gradient) are loaded for the elements this pass owns
-      T v[NIN], o[NOUT];
-      v[IA] = a;
-      v[IX] = x;
-      const int reg = Fn::classify(v, tab, xt);
-      bool mine = true;
-      if constexpr (PASS != 0) {
-        const bool second = Fn::fp64_pass(reg, v, p.out_mask, tab, xt);
-        mine = PASS == 2 ? second : !second;
-      }
-      if (mine) {
-#pragma unroll
-        for (int q = 0; q < NIN; ++q)
-          if (q != IA && q != IX)
-            v[q] = load_as<TS, T>(p.in_ptr[q] + ((int64_t)r * p.in_s0[q] + col * p.in_s1[q]) * (int64_t)sizeof(TS));
-        if constexpr (PASS == 0) Fn::eval(reg, v, o, p.out_mask, tab, xt);
-        else Fn::template eval_pass<PASS>(reg, v, o, p.out_mask, tab, xt);
-      }
-      const bool take = mine && rv;
-      const unsigned any = __ballot_sync(0xffffffffu, take);
       const int sj = jj % S;
-      own[sj * 32 + lane] = take;
+      if (PASS == 2 && !((cmask >> jj) & 1u)) {  // no second-pass element in this column (warp-uniform)
+        own[sj * 32 + lane] = 0;
+      } else {
+        const T x = load_as<TS, T>(p.in_ptr[IX] + col * p.in_s1[IX] * (int64_t)sizeof(TS));
+        const double* xt = p.tab_cols + col * N1;  // every lane reads the same entry
+        // classify and fp64_pass read only the two table inputs; the others
+        // (e.g. an upstream gradient) are loaded for the elements this pass owns
+        T v[NIN], o[NOUT];
+        v[IA] = a;
+        v[IX] = x;
+        const int reg = Fn::classify(v, tab, xt);
+        bool mine = true;
+        if constexpr (PASS != 0) {
+          const bool second = Fn::fp64_pass(reg, v, p.out_mask, tab, xt);
+          mine = PASS == 2 ? second : !second;
+          if constexpr (PASS == 1) {
+            if (__any_sync(0xffffffffu, second)) cmask |= 1u << jj;
+          }
+        }
+        if (mine) {
 #pragma unroll
-      for (int q = 0; q < NOUT; ++q) {
-        if (!(p.out_mask & (1u << q))) continue;
-        const int kind = p.out_kind[q];
-        if (kind == kOutFull) {
-          if (take) so[(q * S + sj) * 33 + lane] = o[q];
-        } else if (kind == kOutRow || kind == kOutAll) {
-          if (take) acc[q * 32] += (double)o[q];
-        } else if (kind == kOutCol) {
-          // the first pass writes every partial, the second adds its own
-          if (PASS != 2 || any) {
-            double s = take ? (double)o[q] : 0.0;
+          for (int q = 0; q < NIN; ++q)
+            if (q != IA && q != IX)
+              v[q] = load_as<TS, T>(p.in_ptr[q] + ((int64_t)r * p.in_s0[q] + col * p.in_s1[q]) * (int64_t)sizeof(TS));
+          if constexpr (PASS == 0) Fn::eval(reg, v, o, p.out_mask, tab, xt);
+          else Fn::template eval_pass<PASS>(reg, v, o, p.out_mask, tab, xt);
+        }
+        const bool take = mine && rv;
+        const unsigned any = __ballot_sync(0xffffffffu, take);
+        own[sj * 32 + lane] = take;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-            if (lane == 0) {
-              double* w = p.ws[q] + (int64_t)rb * p.cols + col;
-              *w = PASS == 2 ? *w + s : s;
+        for (int q = 0; q < NOUT; ++q) {
+          if (!(p.out_mask & (1u << q))) continue;
+          const int kind = p.out_kind[q];
+          if (kind == kOutFull) {
+            if (take) so[(q * S + sj) * 33 + lane] = o[q];
+          } else if (kind == kOutRow || kind == kOutAll) {
+            if (take) acc[q * 32] += (double)o[q];
+          } else if (kind == kOutCol) {
+            // the first pass writes every partial, the second adds its own
+            if (PASS != 2 || any) {
+              double s = take ? (double)o[q] : 0.0;
+#pragma unroll
+              for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+              if (lane == 0) {
+                double* w = p.ws[q] + (int64_t)rb * p.cols + col;
+                *w = PASS == 2 ? *w + s : s;
+              }
             }
           }
         }
@@ -240,6 +257,9 @@ __global__ void __launch_bounds__(kBlock, PASS == 1 ? 4 : SweepMinBlocks<Fn>::va
         }
         __syncwarp();
       }
+    }
+    if constexpr (PASS == 1) {
+      if (lane == 0) p.colmask[task] = cmask;
     }
 #pragma unroll
     for (int q = 0; q < NOUT; ++q) {
@@ -311,10 +331,12 @@ int32_t launch_sweep(const Canon& c, bool transpose, const tsb_tensor* out, uint
   sp += align256(p.rows * 4);
   p.tab_rows = reinterpret_cast<double*>(sp);
   p.tab_cols = p.tab_rows + p.rows * Fn::NAUX0;
+  sp += align256((p.rows + p.cols) * kSweepTabMax * 8);
+  p.colmask = reinterpret_cast<uint32_t*>(sp);
   p.counter = reinterpret_cast<int32_t*>(wp + used + sweep_scratch_bytes(p.rows, p.cols) - 256);
 
-  const unsigned sgrid = (unsigned)((p.rows + kRankBlock - 1) / kRankBlock + (p.cols + kRankBlock - 1) / kRankBlock);
-  sweep_setup_kernel<Fn, TS><<<sgrid, kRankBlock, 0, stream>>>(p);
+  const unsigned sgrid = (unsigned)((p.rows + 31) / 32 + (p.cols + kBlock - 1) / kBlock);
+  sweep_setup_kernel<Fn, TS><<<sgrid, kBlock, 0, stream>>>(p);
   count_launches(1);
   int32_t st = check_launch("sweep set-up kernel launch");
   if (st) return st;
@@ -341,18 +363,15 @@ int32_t launch_sweep(const Canon& c, bool transpose, const tsb_tensor* out, uint
     if (!(p.out_mask & (1u << o))) continue;
     const int kind = p.out_kind[o];
     if (kind == kOutRow) {
-      const unsigned g = (unsigned)((p.rows + kBlock - 1) / kBlock);
-      finalize_kernel<TS><<<g, kBlock, 0, stream>>>(p.ws[o], p.rows, p.n_chunks, p.rows, p.out_ptr[o], p.out_s0[o]);
+      launch_finalize<TS>(p.ws[o], p.rows, p.n_chunks, p.rows, p.out_ptr[o], p.out_s0[o], stream);
     } else if (kind == kOutCol) {
-      const unsigned g = (unsigned)((p.cols + kBlock - 1) / kBlock);
-      finalize_kernel<TS><<<g, kBlock, 0, stream>>>(p.ws[o], p.cols, p.n_row_blocks, p.cols, p.out_ptr[o],
-                                                    p.out_s1[o]);
+      launch_finalize<TS>(p.ws[o], p.cols, p.n_row_blocks, p.cols, p.out_ptr[o], p.out_s1[o], stream);
     } else if (kind == kOutAll) {
       finalize_all_kernel<TS><<<1, kBlock, 0, stream>>>(p.ws[o], ntasks, p.out_ptr[o]);
+      count_launches(1);
     } else {
       continue;
     }
-    count_launches(1);
     st = check_launch("finalize kernel launch");
     if (st) return st;
   }

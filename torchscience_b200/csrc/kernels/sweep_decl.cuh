@@ -35,9 +35,9 @@ struct SplitOptIn<Fn, decltype((void)Fn::SPLIT, void())> {
 };
 
 constexpr int kSweepCols = 32;             // columns per task
+static_assert(kSweepCols == 32, "a task's column mask is one 32-bit word");
 constexpr int kSweepStage = 4;             // full-output columns staged per store
 constexpr int64_t kSweepMaxRows = 16384;   // the rank sort is O(rows^2): larger grids use reduce2d_kernel
-constexpr int kRankBlock = 64;
 
 // Per-row / per-column table entries the sweep keeps in its workspace (a
 // functor's NAUX0, NAUX1 must not exceed this many doubles).
@@ -45,11 +45,14 @@ constexpr int kSweepTabMax = 16;
 
 // Scratch the sweep needs beyond the reduced outputs' partial sums, for a grid
 // of n0 x n1 (either orientation): the row order (int32 per sorted row), the
-// row and column tables (kSweepTabMax doubles per row and per column) and the
-// task counter.
+// row and column tables (kSweepTabMax doubles per row and per column), one
+// 32-bit column mask per task (the columns a split sweep's second pass
+// visits; tasks are 32 rows x kSweepCols = 32 columns) and the task counters.
+inline int64_t sweep_task_count(int64_t n0, int64_t n1) { return ((n0 + 31) / 32) * ((n1 + 31) / 32); }
 inline int64_t sweep_scratch_bytes(int64_t n0, int64_t n1) {
   const int64_t rows = n0 > n1 ? n0 : n1;
-  return ((rows * 4 + 255) & ~int64_t(255)) + (((n0 + n1) * kSweepTabMax * 8 + 255) & ~int64_t(255)) + 256;
+  return ((rows * 4 + 255) & ~int64_t(255)) + (((n0 + n1) * kSweepTabMax * 8 + 255) & ~int64_t(255)) +
+         ((sweep_task_count(n0, n1) * 4 + 255) & ~int64_t(255)) + 256;
 }
 
 }  // namespace tsb
