@@ -546,6 +546,10 @@ def our_arm(args):
             "unit": "Gelem/s",
             "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h,
+            # the host link's rate over the step in each direction: the copies of g in and of P out
+            # (134 MB each on the grid) bound the end-to-end step, the kernels overlapping them
+            "h2d_gb_s": h2d / (t_e2e / args.steps) / 1e9,
+            "d2h_gb_s": d2h / (t_e2e / args.steps) / 1e9,
         },
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
@@ -683,6 +687,124 @@ def _max_rel(lo, hi, floor=1e-30):
     return ((lo - hi).abs() / hi.abs())[m].max().item() if bool(m.any()) else 0.0
 
 
+def _err_stats(mixed, fp64, mask):
+    """Max and median of |mixed - fp64| / |fp64| over `mask` and the normal
+    float32 range of the FP64 value (numpy arrays)."""
+    import numpy as np
+
+    m = mask & np.isfinite(fp64) & np.isfinite(mixed) & (np.abs(fp64) > 1.2e-38) & (np.abs(fp64) < 3e38)
+    if not m.any():
+        return {"n": 0}
+    e = np.abs(mixed[m] - fp64[m]) / np.abs(fp64[m])
+    return {"n": int(m.sum()), "max": float(e.max()), "median": float(np.median(e))}
+
+
+def error_tables(sf, dev, gen, U, LU):
+    """Per-function, per-region error tables of the mixed kernels against the
+    FP64 kernels (at the same float32 inputs).  The regions restate the
+    kernels' classification in numpy: the method, and whether the mixed kernel
+    evaluates the element in FP32 or declines it to FP64."""
+    import numpy as np
+
+    ops = torch.ops.torchscience
+    out = {}
+
+    # --- regularized_gamma_p on the configuration-2 grid, every 4th row
+    a, x = make_inputs(0)[:2]
+    a32, x32 = a[::4].float(), x.float()
+    A32 = a32.expand(a32.shape[0], x32.shape[1]).contiguous().to(dev)
+    X32 = x32.expand(a32.shape[0], x32.shape[1]).contiguous().to(dev)
+    A64, X64 = A32.double(), X32.double()
+    with torch.no_grad():
+        p32 = ops.regularized_gamma_p(A32, X32).double().cpu().numpy().ravel()
+        p64 = ops.regularized_gamma_p(A64, X64).cpu().numpy().ravel()
+        ga32, gx32 = [t.double().cpu().numpy().ravel() for t in
+                      ops.regularized_gamma_p_backward(torch.ones_like(A32), A32, X32)]
+        ga64, gx64 = [t.cpu().numpy().ravel() for t in
+                      ops.regularized_gamma_p_backward(torch.ones_like(A64), A64, X64)]
+    an, xn = A64.cpu().numpy().ravel(), X64.cpu().numpy().ravel()
+    lam = xn / (an + 1.0)
+    ser = xn < an + 1.0
+    sat = (p64 == 0.0) | (p64 == 1.0)
+    regions = {
+        "saturated (P = 0 or 1)": sat,
+        "series, x/(a+1) < 0.35 (FP32)": ~sat & ser & (an >= 1) & (lam < 0.35),
+        "series, 0.35 <= x/(a+1) < 0.7 (FP32)": ~sat & ser & (an >= 1) & (lam >= 0.35) & (lam < 0.7),
+        "series, x/(a+1) >= 0.7, transition (FP64)": ~sat & ser & (an >= 1) & (lam >= 0.7),
+        "series, a < 1 (FP32 where ln x < psi(a+1))": ~sat & ser & (an < 1),
+        "fraction, x/(a+1) <= 1.5, transition (FP64)": ~sat & ~ser & (lam <= 1.5),
+        "fraction, 1.5 < x/(a+1) <= 3 (FP64)": ~sat & ~ser & (lam > 1.5) & (lam <= 3),
+        "fraction, x/(a+1) > 3, x >= 20 (FP32 expansion)": ~sat & ~ser & (lam > 3) & (xn >= 20),
+        "fraction, x/(a+1) > 3, x < 20 (FP64)": ~sat & ~ser & (lam > 3) & (xn < 20),
+    }
+    out["regularized_gamma_p"] = {
+        name: {"fraction_of_elements": float(m.mean()), "P": _err_stats(p32, p64, m),
+               "dP/da": _err_stats(ga32, ga64, m), "dP/dx": _err_stats(gx32, gx64, m)}
+        for name, m in regions.items()}
+
+    # --- Bessel J, Y, I, K of real order on configuration-3 points
+    n = 1 << 22
+    nu32, z32 = U(n, 0.0, 20.0).float(), LU(n, 1e-3, 1e3).float()
+    one32 = torch.ones(n, device=dev, dtype=torch.float32)
+    nn, zz = nu32.double().cpu().numpy(), z32.double().cpu().numpy()
+    def dz(fn, nu, z):  # d/dz alone (grad_n not requested), as autograd asks for it
+        zr = z.clone().requires_grad_(True)
+        return torch.autograd.grad(fn(nu, zr), zr, torch.ones_like(zr))[0]
+
+    for name in ("bessel_j", "bessel_y", "modified_bessel_i", "modified_bessel_k"):
+        fn = getattr(sf, name)
+        with torch.no_grad():
+            v32 = fn(nu32, z32).double().cpu().numpy()
+            v64 = fn(nu32.double(), z32.double()).cpu().numpy()
+        d32 = dz(fn, nu32, z32).double().cpu().numpy()
+        d64 = dz(fn, nu32.double(), z32.double()).cpu().numpy()
+        series = zz < 2.0
+        large = (zz >= 25.0) & ((name in ("modified_bessel_i", "modified_bessel_k")) | (nn < zz))
+        mid = ~series & ~large
+        if name in ("bessel_j", "bessel_y"):
+            # the mixed kernels' decline rule: |C| >= 0.3 M (value) with M^2 = C^2 + (C'/w)^2, w = sqrt(1 - (nu/x)^2)
+            r = np.minimum(nn / zz, 1.0)
+            w2 = np.maximum(1.0 - r * r, 1e-300)
+            m2 = v64 ** 2 + d64 ** 2 / w2
+            osc = nn < zz
+            kept_v = ~osc | (v64 ** 2 >= 0.09 * m2)
+            kept_d = ~osc | (d64 ** 2 >= 0.09 * w2 * m2)
+            regs = {
+                "series, x < 2 (FP32)": (series, series),
+                "Steed, 2 <= x < 25 or nu >= x (FP32 away from zeros)": (mid & kept_v, mid & kept_d),
+                "Steed, next to a zero (declined to FP64)": (mid & ~kept_v, mid & ~kept_d),
+                "Hankel, x >= 25 (FP32 away from zeros)": (large & kept_v, large & kept_d),
+                "Hankel, next to a zero (declined to FP64)": (large & ~kept_v, large & ~kept_d),
+            }
+            if name == "bessel_y":
+                regs["series, x < 2 (FP32)"] = (series, series)
+        else:
+            regs = {
+                "series, x < 2 (FP32; K by Temme's series in FP64)": (series, series),
+                "Steed / Temme CF2, 2 <= x < 25 (FP32, recurrence FP64)": (mid, mid),
+                "Hankel, x >= 25 (FP32, recurrence FP64)": (large, large),
+            }
+        out[name] = {rn: {"fraction_of_elements": float(mv.mean()), "value": _err_stats(v32, v64, mv),
+                          "d/dx": _err_stats(d32, d64, md)} for rn, (mv, md) in regs.items()}
+        out[name]["all"] = {"value": _err_stats(v32, v64, np.ones(n, bool)),
+                            "d/dx": _err_stats(d32, d64, np.ones(n, bool))}
+
+    # --- K(m), E(m)
+    m32 = U(n, 0.0, 1.0 - 1e-9).float()
+    mm = m32.double().cpu().numpy()
+    for name in ("complete_legendre_elliptic_integral_k", "complete_legendre_elliptic_integral_e"):
+        fn, bw = getattr(ops, name), getattr(ops, name + "_backward")
+        with torch.no_grad():
+            v32 = fn(m32).double().cpu().numpy()
+            v64 = fn(m32.double()).cpu().numpy()
+            d32 = bw(one32, m32).double().cpu().numpy()
+            d64 = bw(one32.double(), m32.double()).cpu().numpy()
+        regs = {"m < 0.9 (AGM)": mm < 0.9, "m >= 0.9 (complementary series)": mm >= 0.9}
+        out[name] = {rn: {"fraction_of_elements": float(mk.mean()), "value": _err_stats(v32, v64, mk),
+                          "d/dm": _err_stats(d32, d64, mk)} for rn, mk in regs.items()}
+    return out
+
+
 def secondary_arm(args):
     """The other benchmark configurations (parity-test cases of the path), timed
     the same way; one JSON line with one entry per function."""
@@ -766,8 +888,13 @@ def secondary_arm(args):
                 with torch.no_grad():
                     row[f"{tag}_fwd_gelem_s"] = _rate(lambda: fn(nu, x), n, S, W, flush)
                 row[f"{tag}_fwd_bwd_gelem_s"] = _rate(fb, n, S, W, flush)
+            import torchscience_b200 as tsb
+
             with torch.no_grad():
+                tsb.unconverged_count(reset=True)
                 row["mixed_max_rel_err_vs_fp64"] = _max_rel(fn(nu32, x32), fn(nu32.double(), x32.double()))
+                # elements of the two forwards whose series or fractions stopped at an iteration cap
+                row["unconverged_elements_fwd"] = tsb.unconverged_count(reset=True)
             row["mixed_speedup_fwd_bwd"] = row["mixed_fwd_bwd_gelem_s"] / row["fp64_fwd_bwd_gelem_s"]
             # fwd + d/dx: read nu, x, g, write y and grad_x (4 B each in float32, 8 in float64)
             row["roofline_mixed"] = roofline(20, row["mixed_fwd_bwd_gelem_s"], f"{name} fwd + backward, float32")
@@ -971,6 +1098,12 @@ def secondary_arm(args):
             res[name] = row
         if ref_cpu is not None:
             res["reference_cpu_threads"] = os.cpu_count()
+    elif args.workload == "errors":
+        desc = ("relative error of the mixed (float32) kernels against the FP64 kernels at the same float32 values, "
+                "per function and evaluation region, for values and first derivatives (the _backward ops with a unit "
+                "upstream gradient, full shape); P on every 4th row of the configuration-2 grid, J/Y/I/K on 2^22 "
+                "configuration-3 points, K and E on 2^22 points m ~ U(0, 1 - 1e-9)")
+        res = error_tables(sf, dev, gen, U, LU)
     print(json.dumps({
         "metric": METRIC, "workload": args.workload, "unit": "Gelem/s", "steps": S, "warmup": W,
         "data": "synthetic, seeded on the device", "config": {"workload": desc, "l2": "flushed between steps"},
@@ -985,7 +1118,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument(
-        "--workload", choices=["p_grid", "c1", "c3", "c4", "c5", "siblings"], default="p_grid",
+        "--workload", choices=["p_grid", "c1", "c3", "c4", "c5", "siblings", "errors"], default="p_grid",
         help="p_grid (default): the headline P(a, x) workload; c1/c3/c4/c5: the other configurations, one GPU; "
              "siblings: the ops beside P and Q, one GPU")
     args = ap.parse_args()

@@ -170,3 +170,46 @@ def test_full_size_properties_config2():
     d = torch.exp(a * torch.log(x) - x - torch.lgamma(a + 1))
     r = (p1 - (p - d)).abs()
     assert r.max().item() <= 1e-12
+
+
+def test_uniform_expansion_window_against_mpmath():
+    """The transition window a >= 20, 0.6 <= x/a <= 1.6, evaluated by Temme's
+    uniform expansion: P, Q (the smaller one directly), dP/da and dP/dx against
+    mpmath at 40 digits, on a fixed grid of a (20 to 1e4, the window's edges
+    included) and x/a (both edges, x = a, and points on either side of the
+    window, where the series and the continued fraction take over).  Bounds as
+    in test_fp64_values_against_mpmath for the values, 1e-10 for dP/da,
+    1e-12 for dP/dx."""
+    import mpmath
+
+    mpmath.mp.dps = 40
+    a_list = [20.0, 20.5, 27.3, 64.0, 150.0, 777.7, 4096.0, 1e4]
+    lam_list = [0.55, 0.6, 0.61, 0.75, 0.9, 0.99, 1.0, 1.01, 1.2, 1.45, 1.59, 1.6, 1.7]
+    a = np.array([av for av in a_list for _ in lam_list])
+    x = np.array([av * lv for av in a_list for lv in lam_list])
+    (p,) = run("regularized_gamma_p", cuda(a), cuda(x))
+    (q,) = run("regularized_gamma_q", cuda(a), cuda(x))
+    ga, gx = run("regularized_gamma_p_backward", cuda(np.ones_like(a)), cuda(a), cuda(x), n_out=2)
+    p, q, ga, gx = [t.cpu().numpy() for t in (p, q, ga, gx)]
+    for i in range(a.size):
+        am, xm = mpmath.mpf(a[i]), mpmath.mpf(x[i])
+        tp = mpmath.gammainc(am, 0, xm, regularized=True)
+        tq = mpmath.gammainc(am, xm, mpmath.inf, regularized=True)
+        small, got = (tp, p[i]) if tp <= tq else (tq, q[i])
+        if small < 1e-300:
+            continue
+        e = abs(got - float(small)) / float(small)
+        bound = 8 * 2.2e-16 * (1 + abs(float(mpmath.log(small)))) + 2e-14
+        assert e <= bound, f"a={a[i]} x={x[i]}: value rel err {e:.3e} > {bound:.3e}"
+        # the derivative of the smaller function, so that 40 digits resolve it
+        if tp <= tq:
+            dpa = mpmath.diff(lambda s: mpmath.gammainc(s, 0, xm, regularized=True), am)
+        else:
+            dpa = -mpmath.diff(lambda s: mpmath.gammainc(s, xm, mpmath.inf, regularized=True), am)
+        dpx = mpmath.exp((am - 1) * mpmath.log(xm) - xm - mpmath.loggamma(am))
+        if abs(dpa) > 1e-290:
+            ea = abs(ga[i] - float(dpa)) / abs(float(dpa))
+            assert ea <= 1e-10, f"a={a[i]} x={x[i]}: dP/da rel err {ea:.3e}"
+        if dpx > 1e-290:
+            ex = abs(gx[i] - float(dpx)) / float(dpx)
+            assert ex <= 1e-12, f"a={a[i]} x={x[i]}: dP/dx rel err {ex:.3e}"

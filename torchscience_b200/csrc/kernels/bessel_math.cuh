@@ -61,6 +61,11 @@ struct BesselK;
 template <>
 struct BesselK<double> {
   static constexpr double EPS = 1.1e-16;
+  // Convergence of a continued fraction judged by its factor's distance
+  // from 1: just over one unit of 1's spacing (2^-52), so that a factor that
+  // settles one ulp above or below 1 ends the loop instead of running to
+  // MAXIT (EPS alone accepts only a factor of exactly 1 or 1 - 2^-53).
+  static constexpr double EPS_RATIO = 2.3e-16;
   static constexpr double FPMIN = 1e-300;
   static constexpr double BIG = 1e280;
   static constexpr int MAXIT = 20000;
@@ -68,6 +73,7 @@ struct BesselK<double> {
 template <>
 struct BesselK<float> {
   static constexpr float EPS = 6e-8f;
+  static constexpr float EPS_RATIO = 1.3e-7f;  // just over one unit of 1's spacing (2^-23), as above
   static constexpr float FPMIN = 1e-35f;
   static constexpr float BIG = 1e35f;
   static constexpr int MAXIT = 20000;
@@ -356,7 +362,7 @@ __device__ inline JY<T> besseljy_pos(T nu, T x) {
       const T del = c * d;
       h *= del;
       if (d < T(0)) isign = -isign;
-      if (fabs(del - T(1)) < eps) break;
+      if (fabs(del - T(1)) < BesselK<T>::EPS_RATIO) break;
     }
     if (i >= BesselK<T>::MAXIT) note_unconverged();
   }
@@ -409,7 +415,7 @@ __device__ inline JY<T> besseljy_pos(T nu, T x) {
       tmp = p * dlr - q * dli;
       q = p * dli + q * dlr;
       p = tmp;
-      if (fabs(dlr - T(1)) + fabs(dli) < eps) break;
+      if (fabs(dlr - T(1)) + fabs(dli) < BesselK<T>::EPS_RATIO) break;
     }
     if (i >= BesselK<T>::MAXIT) note_unconverged();
   }
@@ -526,7 +532,7 @@ __device__ inline IK<T> besselik_pos(T nu, T x, bool& scaled) {
           c = b + T(1) / c;
           const T del = c * d;
           h *= del;
-          if (fabs(del - T(1)) < eps) break;
+          if (fabs(del - T(1)) < BesselK<T>::EPS_RATIO) break;
         }
         if (i >= BesselK<T>::MAXIT) note_unconverged();
       }

@@ -178,15 +178,18 @@ __device__ inline BesselNuDerivs bessel_nu_derivs(double nu, double x, const BV<
   return o;
 }
 
-// Value (+ d/dx) in the mixed kernels: FP32 in the kBsSeries region, and for
-// I and K (which have no zeros, so FP32 keeps its relative accuracy) also in
-// the Steed and Hankel regions, with the order recurrences in FP64; FP64
-// otherwise.  Non-finite FP32 results (values at the edge of FP32 range) are
-// redone in FP64.
+// Value (+ d/dx) in the mixed kernels: FP32 in the kBsSeries region; for K
+// (no zeros) also in the Steed (Temme's CF2) and Hankel regions, and for I
+// where it is Hankel's expansion (x >= 25 and x >= ν²/2), with the order
+// recurrences in FP64; FP64 otherwise.  Measured against the FP64 kernels on
+// configuration-3 points, Steed's CF1 for J, Y and I carries up to ~2e-5 in
+// FP32, so those stay FP64.  Non-finite FP32 results (values at the edge of
+// FP32 range) are redone in FP64.
 template <typename T, int KIND>
 __device__ __forceinline__ BV<T> bessel_value(int region, T nu, T x) {
   if constexpr (std::is_same<T, float>::value) {
-    const bool fp32 = region == kBsSeries || ((KIND == kBI || KIND == kBK) && (region == kBsMid || region == kBsLarge));
+    const bool fp32 = region == kBsSeries || (KIND == kBK && (region == kBsMid || region == kBsLarge)) ||
+                      (KIND == kBI && region == kBsLarge && x >= 0.5f * nu * nu);
     if (fp32) {
       const BV<float> f = bessel_eval<float, KIND>(nu, x);
       if (isfinite(f.v) && isfinite(f.d)) return f;
@@ -198,8 +201,8 @@ __device__ __forceinline__ BV<T> bessel_value(int region, T nu, T x) {
   }
 }
 
-// J and Y in the mixed kernels' Steed and Hankel regions: FP32, with the
-// elements next to a zero of the requested quantity declined to the FP64
+// J and Y in the mixed kernels' Hankel region (x >= 25, ν < x): FP32, with
+// the elements next to a zero of the requested quantity declined to the FP64
 // evaluator (the map kernel's rescue list).  Near a zero the FP32 result keeps
 // its absolute accuracy, about 3 ulp of the local modulus M, but not its
 // relative accuracy.  With the Debye phase rate w = sqrt(1 - (ν/x)²) the
@@ -219,7 +222,7 @@ __device__ __forceinline__ bool bessel_fp32_kept(float nu, float x, float v, flo
 template <typename T, int KIND>
 __device__ __forceinline__ bool bessel_first(int region, T nu, T x, bool deriv, BV<T>& out) {
   if constexpr (std::is_same<T, float>::value && (KIND == kBJ || KIND == kBY)) {
-    if ((region == kBsMid || region == kBsLarge) && nu >= 0.0f && x > 0.0f) {
+    if (region == kBsLarge && nu >= 0.0f && x > 0.0f) {
       const BV<float> f = bessel_eval<float, KIND>(nu, x);
       if (!bessel_fp32_kept(nu, x, f.v, f.d, deriv)) return false;
       out = f;
@@ -426,11 +429,14 @@ template <int KIND, int ORDER>
 __device__ __forceinline__ int bessel_int_classify(double z) {
   return bessel_classify<KIND>((double)ORDER, z);
 }
+// J1 runs the order-0/1 path, of uniform cost: one region (no staging).
+template <int KIND>
+constexpr int kBesselIntRegions = KIND == kBJ ? 1 : kBsRegions;
 
 template <int KIND, int ORDER, typename T_>
 struct BesselIntFwd {
   using T = T_;
-  static constexpr int NIN = 1, NOUT = 1, R = kBsRegions;
+  static constexpr int NIN = 1, NOUT = 1, R = kBesselIntRegions<KIND>;
   static constexpr bool REDUCE = false;
   __device__ static int classify(const T* in) { return bessel_int_classify<KIND, ORDER>((double)in[0]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
@@ -440,7 +446,7 @@ struct BesselIntFwd {
 template <int KIND, int ORDER, typename T_>
 struct BesselIntBwd {  // in = {grad, z}
   using T = T_;
-  static constexpr int NIN = 2, NOUT = 1, R = kBsRegions;
+  static constexpr int NIN = 2, NOUT = 1, R = kBesselIntRegions<KIND>;
   static constexpr bool REDUCE = false;
   __device__ static int classify(const T* in) { return bessel_int_classify<KIND, ORDER>((double)in[1]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {
@@ -450,7 +456,7 @@ struct BesselIntBwd {  // in = {grad, z}
 template <int KIND, int ORDER, typename T_>
 struct BesselIntBwdBwd {  // in = {gg, grad, z}: {gg·f'(z), gg·grad·f''(z)}
   using T = T_;
-  static constexpr int NIN = 3, NOUT = 2, R = kBsRegions;
+  static constexpr int NIN = 3, NOUT = 2, R = kBesselIntRegions<KIND>;
   static constexpr bool REDUCE = true;
   __device__ static int classify(const T* in) { return bessel_int_classify<KIND, ORDER>((double)in[2]); }
   __device__ static void eval(int, const T* in, T* out, uint32_t) {

@@ -24,6 +24,7 @@
 
 #include "fits.cuh"
 #include "gamma_math.cuh"
+#include "temme_fits.cuh"
 
 namespace tsb {
 
@@ -180,8 +181,8 @@ struct IgPre {
 // the digits that t = (x-a)/a rounds away when x << a.
 __device__ inline double igamma_log_prefix_d(double a, double x, const IgPre& P) {
   if (a < 10.0) return a * P.lx() - x - P.lg();
-  const double t = (x - a) / a;
-  const double core = fabs(t) < 0.5 ? a * log1pmx_d(t) : a * log(x / a) - (x - a);
+  const double t = (x - a) * P.ra();  // (x - a)/a to an ulp of t, which moves ln D by ~a t² 2^-53
+  const double core = fabs(t) < 0.5 ? a * log1pmx_d(t) : a * log(x * P.ra()) - (x - a);
   return core - P.lg();
 }
 
@@ -400,19 +401,21 @@ __device__ __forceinline__ int igamma_classify(double ad, double xd, const IgPre
   // threshold e^-745.  Larger a (or x) skip the test: the FP64 evaluator
   // forms ln D accurately and saturates there.
   const bool can_saturate = a < 1e5f && x < 1e5f;
-  const float lratio = fmaxf(0.0f, __logf(a / x));
-  const float lam = x / (a + 1.0f);
-  if (x < a + 1.0f) {
+  // ln(a/x) and the ratio λ = x/(a+1) without divisions: the logarithms come
+  // from the tables, and λ is compared as x against multiples of a + 1
+  const float lratio = fmaxf(0.0f, P.laf() - P.lxf());
+  const float a1 = a + 1.0f;
+  if (x < a1) {
     // P <= D·(a+1)/(a+1-x) ~ D·a.
     if (can_saturate && lnd + P.la1f() + lratio < -760.0f) return kIgSat0;
-    if (a < 1.0f) return lam < 0.1f ? kIgSmallA0 : kIgSmallA;
-    return lam < 0.01f ? kIgS00 : lam < 0.1f ? kIgS0 : lam < 0.35f ? kIgS1 : lam < 0.7f ? kIgS2
+    if (a < 1.0f) return x < 0.1f * a1 ? kIgSmallA0 : kIgSmallA;
+    return x < 0.01f * a1 ? kIgS00 : x < 0.1f * a1 ? kIgS0 : x < 0.35f * a1 ? kIgS1 : x < 0.7f * a1 ? kIgS2
                                                                                 : igamma_transition_bucket(false, a);
   }
   // Q = a D F with F <= 1/(x+1-a) <= 1.
   if (can_saturate && lnd + P.laf() + lratio < -760.0f) return kIgSat1;
   if (mixed_fwd && a < 1.0f) return kIgCa;
-  return lam > 10.0f ? kIgC00 : lam > 3.0f ? kIgC0 : lam > 1.5f ? kIgC1 : igamma_transition_bucket(true, a);
+  return x > 10.0f * a1 ? kIgC00 : x > 3.0f * a1 ? kIgC0 : x > 1.5f * a1 ? kIgC1 : igamma_transition_bucket(true, a);
 }
 __device__ __forceinline__ int igamma_classify(double ad, double xd, bool mixed_fwd = false) {
   return igamma_classify(ad, xd, IgPre{nullptr, nullptr, ad, xd}, mixed_fwd);
@@ -437,6 +440,57 @@ __device__ inline double igamma_q_small_a_d(double a, double x, double lx) {
     if (n >= 80) note_unconverged();
   }
   return -expm1(e) - exp(e) * a * T;
+}
+
+// Temme's uniform asymptotic expansion (DLMF 8.12.3-8.12.4, 8.12.10), for
+// a >= TEMME_A_MIN and TEMME_LAM_LO <= x/a <= TEMME_LAM_HI: the transition
+// x ~ a, where the series and the continued fraction need a number of terms
+// growing like √a, in a fixed number of operations.  With u = x/a - 1 and
+// η = sign(u) sqrt(-2 (ln(1+u) - u)),
+//   Q = ½ erfc(η sqrt(a/2)) + R,  P = ½ erfc(-η sqrt(a/2)) - R,
+//   R = e^(-aη²/2) / sqrt(2πa) · S,  S = Σ c_k(η) a^-k,
+// the smaller of P and Q computed directly and the other as 1 minus it.
+// The c_k are Taylor series in η (temme_fits.cuh, generated and checked
+// against mpmath by fits/gen_temme.py).  First derivatives: ∂P/∂x = D a/x with
+// D = e^(-aη²/2) / (sqrt(2πa) Γ*(a)), Γ*(a) = e^μ(a) (DLMF 5.11.3); with
+// dη/da = -(u/η)/a,
+//   ∂P/∂a = e^(-aη²/2)/sqrt(2πa) · [η/2 - u/η - S (ln(1+u) - 1/(2a)) + (Sk + Se u/η)/a],
+// Se = Σ c_k'(η) a^-k, Sk = Σ k c_k(η) a^-k.
+__device__ __forceinline__ bool igamma_temme_applies(double a, double x) {
+  return a >= fits::TEMME_A_MIN && x >= fits::TEMME_LAM_LO * a && x <= fits::TEMME_LAM_HI * a;
+}
+
+template <int ORDER>
+__device__ inline IgammaOut igamma_temme_d(double a, double x, const IgPre& P) {
+  IgammaOut o;
+  o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
+  const double r = P.ra();
+  const double u = (x - a) * r;
+  const double lm = log1pmx_d(u);  // ln(1+u) - u = -η²/2
+  const double eta = u == 0.0 ? 0.0 : copysign(sqrt(-2.0 * lm), u);
+  double S, Se, Sk;
+  fits::temme_sums<(ORDER >= 1)>(eta, r, S, Se, Sk);
+  const double pref = exp(fma(a, lm, -0.5 * (1.8378770664093453 + P.la())));  // e^(-aη²/2) / sqrt(2πa)
+  const double s = eta * sqrt(0.5 * a);
+  const double R = pref * S;
+  if (eta >= 0.0) {
+    o.q = fma(0.5, erfc(s), R);
+    o.p = 1.0 - o.q;
+  } else {
+    o.p = fma(0.5, erfc(-s), -R);
+    o.q = 1.0 - o.p;
+  }
+  if (ORDER >= 1) {
+    const double rue = eta == 0.0 ? 1.0 : u / eta;
+    o.pa = pref * (0.5 * eta - rue - S * (log1p(u) - 0.5 * r) + r * fma(Se, rue, Sk));
+    // D a/x = pref e^-μ / (1+u); e^-μ by its Taylor series (μ <= 1/(12 a) <= 0.0042)
+    const double mu = stirling_mu_d(a);
+    double em = 1.0;  // 1 - μ(1 - μ/2(1 - μ/3(...))), seven terms: the rest is below 1e-20
+#pragma unroll
+    for (int k = 7; k >= 1; --k) em = fma(-mu * (1.0 / k), em, 1.0);
+    o.px = pref * em / (1.0 + u);
+  }
+  return o;
 }
 
 // FP64 evaluation.  ORDER 0: p,q; 1: + pa, px; 2: + paa, pax, pxx.
@@ -465,11 +519,14 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
     o.q = 1.0;
     return o;
   }
+  if (ORDER <= 1 && igamma_temme_applies(a, x)) return igamma_temme_d<ORDER>(a, x, P);
   const double lnD = igamma_log_prefix_d(a, x, P);
   const double lx = P.lx();
   // ∂P/∂x = x^(a-1) e^{-x} / Γ(a) = D·a/x
   if (x < a + 1.0) {
-    if (lnD + log1p(a) < -760.0) {
+    // P <= D (a+1): below e^-760 it underflows (ln(a+1) from the table's float
+    // value: the test has a margin of 15 to the underflow threshold e^-745)
+    if (lnD + (double)P.la1f() < -760.0) {
       o.p = 0.0;
       o.q = 1.0;
       return o;
