@@ -24,27 +24,40 @@ def test_ordinary_inputs_count_nothing():
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-def test_a_series_past_its_cap_is_counted(dtype):
-    # P(a, x) at a = x = 1e9 needs ~1e5 series terms; the cap is 2000
+def test_a_fraction_past_its_cap_is_counted(dtype):
+    # I_x(a, b) at x = 1/2, a = b = 1e9 needs ~2e4 terms of its continued
+    # fraction next to the swap point; the cap is 4000 terms
+    x = torch.tensor([0.5, 0.3], device="cuda", dtype=dtype)
     a = torch.tensor([1e9, 2.0], device="cuda", dtype=dtype)
-    x = torch.tensor([1e9, 1.0], device="cuda", dtype=dtype)
+    b = torch.tensor([1e9, 3.0], device="cuda", dtype=dtype)
     tsb.unconverged_count(reset=True)
-    p = sf.regularized_gamma_p(a, x)
+    v = sf.incomplete_beta(x, a, b)
     n = tsb.unconverged_count(reset=True)
     assert n == 1, n
-    assert bool(torch.isfinite(p).all())
+    assert bool(torch.isfinite(v).all())
     assert tsb.unconverged_count() == 0  # the reset took effect
 
 
+def test_the_transition_at_large_a_reaches_no_cap():
+    # P(a, x) at a = x = 1e9 would need ~1e5 series terms; the uniform
+    # asymptotic expansion evaluates it in a fixed number of operations
+    a = torch.tensor([1e9, 1e9 * 0.999, 1e9 * 1.001], device="cuda", dtype=torch.float64)
+    tsb.unconverged_count(reset=True)
+    p = sf.regularized_gamma_p(a.new_full((3,), 1e9), a)
+    assert tsb.unconverged_count(reset=True) == 0
+    assert bool(torch.isfinite(p).all())
+
+
 def test_check_convergence_warns_and_raises():
+    x = torch.tensor([0.5], device="cuda", dtype=torch.float64)
     a = torch.tensor([1e9], device="cuda", dtype=torch.float64)
     with pytest.warns(tsb.ConvergenceWarning):
         with tsb.check_convergence("warn"):
-            sf.regularized_gamma_q(a, a)
+            sf.incomplete_beta(x, a, a)
     with pytest.raises(RuntimeError, match="iteration cap"):
         with tsb.check_convergence("raise"):
-            sf.regularized_gamma_q(a, a)
+            sf.incomplete_beta(x, a, a)
     with warnings.catch_warnings():
         warnings.simplefilter("error")
         with tsb.check_convergence("warn"):
-            sf.regularized_gamma_q(a * 0 + 3.0, a * 0 + 2.0)
+            sf.incomplete_beta(x * 0 + 0.3, a * 0 + 2.0, a * 0 + 3.0)

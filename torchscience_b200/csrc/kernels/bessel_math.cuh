@@ -289,14 +289,16 @@ __device__ inline void hankel_sums(T nu, T x, T& P, T& Q, T& Sp, T& Sm) {
   }
 }
 
-// J_ν, J'_ν, Y_ν, Y'_ν for ν >= 0, 0 < x < inf.
-template <typename T, bool NEED_Y>
+// J_ν, J'_ν, Y_ν, Y'_ν for ν >= 0, 0 < x < inf.  NEED_J false: only Y
+// (the series and Hankel regions then skip J's sum and recurrence; Steed's
+// method yields both together).
+template <typename T, bool NEED_Y, bool NEED_J = true>
 __device__ inline JY<T> besseljy_pos(T nu, T x) {
   const T eps = BesselK<T>::EPS, fpmin = BesselK<T>::FPMIN, pi = T(CUDART_PI);
   JY<T> r;
-  r.y = r.yp = T(0);
+  r.j = r.jp = r.y = r.yp = T(0);
   if (x < T(2)) {
-    bessel_series<T>(nu, x, T(-1), r.j, r.jp);
+    if (NEED_J) bessel_series<T>(nu, x, T(-1), r.j, r.jp);
     if (NEED_Y) {
       const int nl = (int)(nu + T(0.5));
       const T mu = nu - T(nl);
@@ -332,9 +334,11 @@ __device__ inline JY<T> besseljy_pos(T nu, T x) {
       c[o][1] = amp * (P * sw + Q * cw);
     }
     T j0 = c[0][0], j1 = c[1][0], y0 = c[0][1], y1 = c[1][1];
-    recur_up_fp64<T>(mu, x, nl, T(1), j0, j1);
-    r.j = j0;
-    r.jp = nu / x * j0 - j1;
+    if (NEED_J) {
+      recur_up_fp64<T>(mu, x, nl, T(1), j0, j1);
+      r.j = j0;
+      r.jp = nu / x * j0 - j1;
+    }
     if (NEED_Y) {
       recur_up_fp64<T>(mu, x, nl, T(1), y0, y1);
       r.y = y0;

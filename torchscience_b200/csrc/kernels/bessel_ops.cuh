@@ -88,7 +88,9 @@ __device__ inline BV<T> bessel_eval(T nu, T x) {
   T v, d;
   if (KIND == kBJ || KIND == kBY) {
     const bool need_y = KIND == kBY || (nu < T(0) && !is_int);
-    const JY<T> r = need_y ? besseljy_pos<T, true>(an, ax) : besseljy_pos<T, false>(an, ax);
+    const bool need_j = KIND == kBJ || (nu < T(0) && !is_int);  // Y_{-a} takes J_a (DLMF 10.4.7)
+    const JY<T> r = !need_y ? besseljy_pos<T, false>(an, ax)
+                            : (need_j ? besseljy_pos<T, true>(an, ax) : besseljy_pos<T, true, false>(an, ax));
     if (nu >= T(0) || is_int) {
       v = KIND == kBJ ? r.j : r.y;
       d = KIND == kBJ ? r.jp : r.yp;
@@ -178,18 +180,18 @@ __device__ inline BesselNuDerivs bessel_nu_derivs(double nu, double x, const BV<
   return o;
 }
 
-// Value (+ d/dx) in the mixed kernels: FP32 in the kBsSeries region; for K
-// (no zeros) also in the Steed (Temme's CF2) and Hankel regions, and for I
-// where it is Hankel's expansion (x >= 25 and x >= ν²/2), with the order
+// Value (+ d/dx) in the mixed kernels: FP32 in the kBsSeries region (J, I, K;
+// Y's series region is Temme's series in FP64 either way); for K (no zeros)
+// also in the Steed (Temme's CF2) and Hankel regions, with the order
 // recurrences in FP64; FP64 otherwise.  Measured against the FP64 kernels on
 // configuration-3 points, Steed's CF1 for J, Y and I carries up to ~2e-5 in
-// FP32, so those stay FP64.  Non-finite FP32 results (values at the edge of
-// FP32 range) are redone in FP64.
+// FP32 and I's Hankel path up to 1.2e-6, so those stay FP64 (J and Y take
+// FP32 in the Hankel region through bessel_first below).  Non-finite FP32
+// results (values at the edge of FP32 range) are redone in FP64.
 template <typename T, int KIND>
 __device__ __forceinline__ BV<T> bessel_value(int region, T nu, T x) {
   if constexpr (std::is_same<T, float>::value) {
-    const bool fp32 = region == kBsSeries || (KIND == kBK && (region == kBsMid || region == kBsLarge)) ||
-                      (KIND == kBI && region == kBsLarge && x >= 0.5f * nu * nu);
+    const bool fp32 = (region == kBsSeries && KIND != kBY) || (KIND == kBK && (region == kBsMid || region == kBsLarge));
     if (fp32) {
       const BV<float> f = bessel_eval<float, KIND>(nu, x);
       if (isfinite(f.v) && isfinite(f.d)) return f;

@@ -197,33 +197,18 @@ def main():
              "namespace tsb {", "namespace fits {", "",
              f"constexpr double TEMME_A_MIN = {A_MIN!r};", f"constexpr double TEMME_LAM_LO = {LAM_LO!r};",
              f"constexpr double TEMME_LAM_HI = {LAM_HI!r};", f"constexpr int TEMME_K = {len(Ck)};", ""]
+    offs = [0]
+    for c in Ck:
+        offs.append(offs[-1] + len(c))
+    lines.append("// c_k(η) = Σ_j TEMME_COEF[TEMME_OFF[k] + j] η^j, j < TEMME_OFF[k+1] - TEMME_OFF[k].")
+    lines.append(f"__device__ const int TEMME_OFF[{len(offs)}] = {{{', '.join(str(o) for o in offs)}}};")
+    lines.append(f"__device__ const double TEMME_COEF[{offs[-1]}] = {{")
     for k, c in enumerate(Ck):
-        lines.append(f"__device__ const double TEMME_C{k}[{len(c)}] = {{")
+        lines.append(f"    // c_{k}")
         lines += [f"    {v!r}," for v in c]
-        lines.append("};")
-    lines += ["",
-              "// S = Σ_k c_k(η) r^k with r = 1/a; when DERIV also Se = Σ_k c_k'(η) r^k and",
-              "// Sk = Σ_k k c_k(η) r^k (so that ∂S/∂a = -r Sk).  Horner in η for each c_k (and",
-              "// its derivative), then in r; every index is a compile-time constant.",
-              "template <bool DERIV>",
-              "__device__ __forceinline__ void temme_sums(double eta, double r, double& S, double& Se, double& Sk) {",
-              "  double c, d;",
-              "  S = Se = Sk = 0.0;"]
-    for k in range(len(Ck) - 1, -1, -1):
-        n = len(Ck[k])
-        lines.append(f"  c = TEMME_C{k}[{n - 1}];")
-        lines.append("  d = 0.0;")
-        lines.append(f"#pragma unroll")
-        lines.append(f"  for (int j = {n - 2}; j >= 0; --j) {{")
-        lines.append("    if (DERIV) d = fma(d, eta, c);")
-        lines.append(f"    c = fma(c, eta, TEMME_C{k}[j]);")
-        lines.append("  }")
-        lines.append("  S = fma(S, r, c);")
-        lines.append("  if (DERIV) {")
-        lines.append("    Se = fma(Se, r, d);")
-        lines.append(f"    Sk = fma(Sk, r, {float(k)!r} * c);")
-        lines.append("  }")
-    lines += ["}", "", "}  // namespace fits", "}  // namespace tsb", ""]
+    lines.append("};")
+
+    lines += ["", "}  // namespace fits", "}  // namespace tsb", ""]
     open(path, "w").write("\n".join(lines))
     print("wrote", path)
 

@@ -76,24 +76,20 @@ enum IgammaAuxA : int {
   kIgA_LGF,     // lgammaf(a+1) in float (classification)
   kIgA_LAF,     // __logf(a)
   kIgA_LA1F,    // __logf(a+1)
-  kIgA_LGFF,    // float-float pairs (packed hi, lo) for the mixed kernels: kIgA_LG,
-  kIgA_LAFF,    //   ln a,
-  kIgA_PRFF,    //   ψ(a) + 1/a,
-  kIgA_PSFF,    //   ψ(a)
+  kIgA_PRFF,    // ψ(a) + 1/a as a packed float-float pair (the mixed kernels' routing test)
   kIgAuxA
 };
 enum IgammaAuxX : int {
   kIgX_LX = 0,  // ln x
   kIgX_RX,      // 1/x
   kIgX_LXF,     // __logf(x)
-  kIgX_LXFF,    // ln x as a packed float-float pair
   kIgAuxX
 };
 
-// Float-float numbers (hi + lo, |lo| <= ulp(hi)/2) for the mixed kernels'
-// prefactor: ln D = a ln x - x - lnΓ(a+1) cancels by up to ~1e4 in the
-// benchmark domain, which plain float cannot carry to 1e-6.  Error-free
-// transformations: TwoSum (Knuth) and the FMA product error.
+// A double split into floats hi + lo (|lo| <= ulp(hi)/2), for the mixed
+// kernels' exponentials: ln D = a ln x - x - lnΓ(a+1) cancels by up to ~1e4
+// in the benchmark domain, so it is formed in FP64 (igamma_lnd_mixed) and its
+// exponential taken as exp(hi)(1 + lo) in float.
 struct IgFF {
   float hi, lo;
 };
@@ -108,20 +104,6 @@ __device__ __forceinline__ double ff_pack(double v) {
 __device__ __forceinline__ IgFF ff_unpack(double d) {
   const long long b = __double_as_longlong(d);
   return IgFF{__int_as_float((int)(b >> 32)), __int_as_float((int)(b & 0xffffffffll))};
-}
-__device__ __forceinline__ IgFF ff_two_sum(float a, float b) {
-  const float s = a + b, bb = s - a;
-  return IgFF{s, (a - (s - bb)) + (b - bb)};
-}
-__device__ __forceinline__ IgFF ff_add(IgFF x, IgFF y) {
-  const IgFF s = ff_two_sum(x.hi, y.hi);
-  return ff_two_sum(s.hi, s.lo + (x.lo + y.lo));
-}
-__device__ __forceinline__ IgFF ff_neg(IgFF x) { return IgFF{-x.hi, -x.lo}; }
-__device__ __forceinline__ IgFF ff_mul_f(IgFF x, float a) {
-  const float p = x.hi * a;
-  const float e = fmaf(x.lo, a, fmaf(x.hi, a, -p));
-  return ff_two_sum(p, e);
 }
 // exp(hi + lo) = exp(hi) (1 + lo) for |lo| << 1.
 __device__ __forceinline__ float ff_exp(IgFF x) { return expf(x.hi) * (1.0f + x.lo); }
@@ -141,16 +123,12 @@ __device__ inline void igamma_aux_a(double a, double* o) {
   o[kIgA_LGF] = lgammaf(af + 1.0f);
   o[kIgA_LAF] = __logf(af);
   o[kIgA_LA1F] = __logf(af + 1.0f);
-  o[kIgA_LGFF] = ff_pack(o[kIgA_LG]);
-  o[kIgA_LAFF] = ff_pack(o[kIgA_LA]);
   o[kIgA_PRFF] = ff_pack(o[kIgA_PSI] + o[kIgA_RA]);
-  o[kIgA_PSFF] = ff_pack(o[kIgA_PSI]);
 }
 __device__ inline void igamma_aux_x(double x, double* o) {
   o[kIgX_LX] = log(x);
   o[kIgX_RX] = 1.0 / x;
   o[kIgX_LXF] = __logf((float)x);
-  o[kIgX_LXFF] = ff_pack(o[kIgX_LX]);
 }
 
 struct IgPre {
@@ -166,11 +144,7 @@ struct IgPre {
   __device__ float laf() const { return A ? (float)A[kIgA_LAF] : __logf((float)a); }
   __device__ float la1f() const { return A ? (float)A[kIgA_LA1F] : __logf((float)a + 1.0f); }
   __device__ double lx() const { return X ? X[kIgX_LX] : log(x); }
-  __device__ IgFF lgff() const { return A ? ff_unpack(A[kIgA_LGFF]) : ff_split(igamma_lg(a)); }
-  __device__ IgFF laff() const { return A ? ff_unpack(A[kIgA_LAFF]) : ff_split(log(a)); }
   __device__ IgFF prff() const { return A ? ff_unpack(A[kIgA_PRFF]) : ff_split(digamma_d(a) + 1.0 / a); }
-  __device__ IgFF psff() const { return A ? ff_unpack(A[kIgA_PSFF]) : ff_split(digamma_d(a)); }
-  __device__ IgFF lxff() const { return X ? ff_unpack(X[kIgX_LXFF]) : ff_split(log(x)); }
   __device__ double rx() const { return X ? X[kIgX_RX] : 1.0 / x; }
   __device__ float lxf() const { return X ? (float)X[kIgX_LXF] : __logf((float)x); }
 };
@@ -460,8 +434,34 @@ __device__ __forceinline__ bool igamma_temme_applies(double a, double x) {
   return a >= fits::TEMME_A_MIN && x >= fits::TEMME_LAM_LO * a && x <= fits::TEMME_LAM_HI * a;
 }
 
+// S = Σ_k c_k(η) r^k with r = 1/a; when DERIV also Se = Σ_k c_k'(η) r^k and
+// Sk = Σ_k k c_k(η) r^k (so that ∂S/∂a = -r Sk): Horner in η for each c_k
+// (and its derivative), then in r.  Loops over the table rather than
+// unrolled code, so that an evaluation fetches a few dozen instructions: the
+// kernels that call it are bound by instruction fetch.
+template <bool DERIV>
+__device__ __forceinline__ void igamma_temme_sums(double eta, double r, double& S, double& Se, double& Sk) {
+  S = Se = Sk = 0.0;
+#pragma unroll 1
+  for (int k = fits::TEMME_K - 1; k >= 0; --k) {
+    const int lo = fits::TEMME_OFF[k], hi = fits::TEMME_OFF[k + 1];
+    double c = fits::TEMME_COEF[hi - 1], d = 0.0;
+#pragma unroll 1
+    for (int j = hi - 2; j >= lo; --j) {
+      if (DERIV) d = fma(d, eta, c);
+      c = fma(c, eta, fits::TEMME_COEF[j]);
+    }
+    S = fma(S, r, c);
+    if (DERIV) {
+      Se = fma(Se, r, d);
+      Sk = fma(Sk, r, (double)k * c);
+    }
+  }
+}
+
+// Out of line: one copy per kernel, fetched only by the warps that take it.
 template <int ORDER>
-__device__ inline IgammaOut igamma_temme_d(double a, double x, const IgPre& P) {
+__device__ __noinline__ IgammaOut igamma_temme_d(double a, double x, const IgPre P) {
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
   const double r = P.ra();
@@ -469,7 +469,7 @@ __device__ inline IgammaOut igamma_temme_d(double a, double x, const IgPre& P) {
   const double lm = log1pmx_d(u);  // ln(1+u) - u = -η²/2
   const double eta = u == 0.0 ? 0.0 : copysign(sqrt(-2.0 * lm), u);
   double S, Se, Sk;
-  fits::temme_sums<(ORDER >= 1)>(eta, r, S, Se, Sk);
+  igamma_temme_sums<(ORDER >= 1)>(eta, r, S, Se, Sk);
   const double pref = exp(fma(a, lm, -0.5 * (1.8378770664093453 + P.la())));  // e^(-aη²/2) / sqrt(2πa)
   const double s = eta * sqrt(0.5 * a);
   const double R = pref * S;
@@ -591,18 +591,23 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
 // a (ln x - ln a) - (x - a) - C(a).  The float continued fraction carries
 // ~1e-6 relative error in Q, which P = 1 - Q scales down by Q/P < 1 in these
 // regions; Q itself takes the FP64 continued fraction.
+// ln D for the mixed evaluators, in FP64 from the per-row / per-column double
+// quantities (a few FP64 operations, far fewer issue slots than the same
+// sum in float-float arithmetic): a ln x - x - lnΓ(a+1) for a < 10, else the
+// direct form a (ln x - ln a) - (x - a) - C(a) (these regions keep x away
+// from a).  Its absolute error, ~1e-16 times the terms' size, is far below
+// what the float evaluation needs.
+__device__ __forceinline__ double igamma_lnd_mixed(float a, float x, const IgPre& P) {
+  const double ad = a, xd = x;
+  return a < 10.0f ? fma(ad, P.lx(), -xd) - P.lg() : fma(ad, P.lx() - P.la(), -(xd - ad)) - P.lg();
+}
+
 template <bool WANT_Q>
 __device__ inline IgammaOut igamma_eval_mf(int region, float a, float x, const IgPre& P) {
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
-  const IgFF lx = P.lxff(), lg = P.lgff();
-  IgFF lnD;
-  if (a < 10.0f) {
-    lnD = ff_add(ff_add(ff_mul_f(lx, a), IgFF{-x, 0.0f}), ff_neg(lg));
-  } else {
-    const IgFF d = ff_add(lx, ff_neg(P.laff()));
-    lnD = ff_add(ff_add(ff_mul_f(d, a), ff_neg(ff_two_sum(x, -a))), ff_neg(lg));
-  }
+  const double lnDd = igamma_lnd_mixed(a, x, P);
+  const IgFF lnD = ff_split(lnDd);
   if (region != kIgC0 && region != kIgC00 && region != kIgCa) {
     float S, S1, S2;
     igamma_series<float, 0>(a, x, S, S1, S2);
@@ -619,7 +624,7 @@ __device__ inline IgammaOut igamma_eval_mf(int region, float a, float x, const I
       igamma_cf<float, 0>(a, x, f, f1, f2);
       F = f;
     }
-    o.q = (double)ff_exp(ff_add(lnD, P.laff())) * F;  // E F, E = D a
+    o.q = (double)ff_exp(ff_split(lnDd + P.la())) * F;  // E F, E = D a
     o.p = 1.0 - o.q;
   }
   return o;
@@ -702,16 +707,9 @@ template <bool WANT_Q>
 __device__ inline IgammaOut igamma_eval_mf1(int region, float a, float x, const IgPre& P) {
   IgammaOut o;
   o.paa = o.pax = o.pxx = 0.0;
-  const IgFF lx = P.lxff(), lg = P.lgff(), la = P.laff();
-  IgFF lnD;
-  if (a < 10.0f) {
-    lnD = ff_add(ff_add(ff_mul_f(lx, a), IgFF{-x, 0.0f}), ff_neg(lg));
-  } else {
-    const IgFF d = ff_add(lx, ff_neg(la));
-    lnD = ff_add(ff_add(ff_mul_f(d, a), ff_neg(ff_two_sum(x, -a))), ff_neg(lg));
-  }
-  const IgFF lnE = ff_add(lnD, la);
-  const IgFF lnEx = ff_add(lnE, ff_neg(lx));  // ln(E/x) = ln ∂P/∂x
+  const double lnDd = igamma_lnd_mixed(a, x, P), lnEd = lnDd + P.la();
+  const IgFF lnD = ff_split(lnDd), lnE = ff_split(lnEd);
+  const IgFF lnEx = ff_split(lnEd - P.lx());  // ln(E/x) = ln ∂P/∂x
   // one exponential per distinct exponent: ∂P/∂x shares ln(E/x) with the
   // expansion's value and a-derivative; the series and the fraction take a
   // second one, of ln D or ln E
@@ -720,7 +718,7 @@ __device__ inline IgammaOut igamma_eval_mf1(int region, float a, float x, const 
   if (region == kIgC0 || region == kIgC00) {
     // Q = (E/x) S, ∂Q/∂a = (E/x) (E1 S + S1), E1 = ln x - ψ(a) (x >= 20 here)
     float S, S1;
-    const IgFF E1 = ff_add(lx, ff_neg(P.psff()));
+    const IgFF E1 = ff_split(P.lx() - P.psi());
     igamma_asym_f(a, x, fabsf(E1.hi), S, S1);
     const float qv = ff_exp_apply(ex, S);
     o.q = qv;
@@ -729,7 +727,7 @@ __device__ inline IgammaOut igamma_eval_mf1(int region, float a, float x, const 
   } else if (region != kIgC1 && region != kIgC2) {
     float S, S1, S2;
     igamma_series<float, 1>(a, x, S, S1, S2);
-    const IgFF L1 = ff_add(lx, ff_neg(P.prff()));
+    const IgFF L1 = ff_split(P.lx() - (P.psi() + P.ra()));
     const IgFFExp ed = ff_exp_split(lnD);
     const float pv = ff_exp_apply(ed, S);
     o.p = pv;
@@ -738,7 +736,7 @@ __device__ inline IgammaOut igamma_eval_mf1(int region, float a, float x, const 
   } else {
     float F, F1, F2;
     igamma_cf<float, 1>(a, x, F, F1, F2);
-    const IgFF E1 = ff_add(lx, ff_neg(P.psff()));
+    const IgFF E1 = ff_split(P.lx() - P.psi());
     const IgFFExp ee = ff_exp_split(lnE);
     const float qv = ff_exp_apply(ee, F);
     o.q = qv;
