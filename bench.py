@@ -76,11 +76,12 @@ def make_inputs(seed: int, dtype=torch.float64):
 
 ELEMS = ROWS * COLS + STRESS
 # From one ncu capture of the dominant kernel (sweep2d_kernel<IgammaFwdGrad<double>, double>, one launch on
-# this grid): dram__bytes_read.sum + dram__bytes_write.sum, and the FP64 pipe's active fraction.
-TRAFFIC_BYTES_P_FWDGRAD = 383.42e6
-PIPE_FRAC_FP64 = 0.368
-TRAFFIC_SOURCE = ("ncu --set full --clock-control none -k regex:sweep2d_kernel -s 1 -c 1 on three launches of "
-                  "regularized_gamma_p_forward_with_grads over this grid (float64)")
+# this grid, the current kernel): dram__bytes_read.sum + dram__bytes_write.sum, and the FP64 pipe's active
+# fraction (sm__pipe_fp64_cycles_active.avg.pct_of_peak_sustained_active).
+TRAFFIC_BYTES_P_FWDGRAD = 385.74e6
+PIPE_FRAC_FP64 = 0.304
+TRAFFIC_SOURCE = ("ncu --set full --clock-control none -k regex:'sweep2d_kernel|stream2d_kernel' -c 4 over one "
+                  "FP64 and one float32 step of this workload; the first captured launch (the FP64 fused forward)")
 
 
 # ------------------------------------------------------------------ clocks
@@ -770,18 +771,21 @@ def error_tables(sf, dev, gen, U, LU):
             kept_v = ~osc | (v64 ** 2 >= 0.09 * m2)
             kept_d = ~osc | (d64 ** 2 >= 0.09 * w2 * m2)
             regs = {
-                "series, x < 2 (FP32)": (series, series),
-                "Steed, 2 <= x < 25 or nu >= x (FP32 away from zeros)": (mid & kept_v, mid & kept_d),
-                "Steed, next to a zero (declined to FP64)": (mid & ~kept_v, mid & ~kept_d),
+                ("series, x < 2 (FP32)" if name == "bessel_j" else "Temme's series, x < 2 (FP64)"): (series, series),
+                "Steed, 2 <= x < 25 or nu >= x (FP64)": (mid, mid),
                 "Hankel, x >= 25 (FP32 away from zeros)": (large & kept_v, large & kept_d),
                 "Hankel, next to a zero (declined to FP64)": (large & ~kept_v, large & ~kept_d),
             }
-            if name == "bessel_y":
-                regs["series, x < 2 (FP32)"] = (series, series)
+        elif name == "modified_bessel_i":
+            regs = {
+                "series, x < 2 (FP32)": (series, series),
+                "Steed's CF1 + Wronskian, 2 <= x < 25 (FP64)": (mid, mid),
+                "x >= 25 (FP64)": (large, large),
+            }
         else:
             regs = {
-                "series, x < 2 (FP32; K by Temme's series in FP64)": (series, series),
-                "Steed / Temme CF2, 2 <= x < 25 (FP32, recurrence FP64)": (mid, mid),
+                "Temme's series, x < 2 (FP64 series, FP64 recurrence)": (series, series),
+                "Temme's CF2, 2 <= x < 25 (FP32, recurrence FP64)": (mid, mid),
                 "Hankel, x >= 25 (FP32, recurrence FP64)": (large, large),
             }
         out[name] = {rn: {"fraction_of_elements": float(mv.mean()), "value": _err_stats(v32, v64, mv),

@@ -173,17 +173,16 @@ def test_full_size_properties_config2():
 
 
 def test_uniform_expansion_window_against_mpmath():
-    """The transition window a >= 20, 0.6 <= x/a <= 1.6, evaluated by Temme's
+    """The transition window a >= 100, 0.6 <= x/a <= 1.6, evaluated by Temme's
     uniform expansion: P, Q (the smaller one directly), dP/da and dP/dx against
-    mpmath at 40 digits, on a fixed grid of a (20 to 1e4, the window's edges
-    included) and x/a (both edges, x = a, and points on either side of the
-    window, where the series and the continued fraction take over).  Bounds as
-    in test_fp64_values_against_mpmath for the values, 1e-10 for dP/da,
-    1e-12 for dP/dx."""
+    mpmath at 50 digits, on a fixed grid of a (the window's edge 100 to 1e4)
+    and x/a (both edges, x = a, and points on either side of the window, where
+    the series and the continued fraction take over).  Bounds as in
+    test_fp64_values_against_mpmath for the values, 1e-10 for dP/da, 1e-12 for
+    dP/dx."""
     import mpmath
 
-    mpmath.mp.dps = 40
-    a_list = [20.0, 20.5, 27.3, 64.0, 150.0, 777.7, 4096.0, 1e4]
+    a_list = [99.9, 100.0, 137.0, 273.0, 640.0, 1500.0, 4096.0, 1e4]
     lam_list = [0.55, 0.6, 0.61, 0.75, 0.9, 0.99, 1.0, 1.01, 1.2, 1.45, 1.59, 1.6, 1.7]
     a = np.array([av for av in a_list for _ in lam_list])
     x = np.array([av * lv for av in a_list for lv in lam_list])
@@ -191,6 +190,13 @@ def test_uniform_expansion_window_against_mpmath():
     (q,) = run("regularized_gamma_q", cuda(a), cuda(x))
     ga, gx = run("regularized_gamma_p_backward", cuda(np.ones_like(a)), cuda(a), cuda(x), n_out=2)
     p, q, ga, gx = [t.cpu().numpy() for t in (p, q, ga, gx)]
+    with mpmath.workdps(50):
+        _check_window(a, x, p, q, ga, gx)
+
+
+def _check_window(a, x, p, q, ga, gx):
+    import mpmath
+
     for i in range(a.size):
         am, xm = mpmath.mpf(a[i]), mpmath.mpf(x[i])
         tp = mpmath.gammainc(am, 0, xm, regularized=True)
@@ -201,7 +207,7 @@ def test_uniform_expansion_window_against_mpmath():
         e = abs(got - float(small)) / float(small)
         bound = 8 * 2.2e-16 * (1 + abs(float(mpmath.log(small)))) + 2e-14
         assert e <= bound, f"a={a[i]} x={x[i]}: value rel err {e:.3e} > {bound:.3e}"
-        # the derivative of the smaller function, so that 40 digits resolve it
+        # the derivative of the smaller function, so that 50 digits resolve it
         if tp <= tq:
             dpa = mpmath.diff(lambda s: mpmath.gammainc(s, 0, xm, regularized=True), am)
         else:

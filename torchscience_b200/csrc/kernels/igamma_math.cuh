@@ -434,32 +434,9 @@ __device__ __forceinline__ bool igamma_temme_applies(double a, double x) {
   return a >= fits::TEMME_A_MIN && x >= fits::TEMME_LAM_LO * a && x <= fits::TEMME_LAM_HI * a;
 }
 
-// S = Σ_k c_k(η) r^k with r = 1/a; when DERIV also Se = Σ_k c_k'(η) r^k and
-// Sk = Σ_k k c_k(η) r^k (so that ∂S/∂a = -r Sk): Horner in η for each c_k
-// (and its derivative), then in r.  Loops over the table rather than
-// unrolled code, so that an evaluation fetches a few dozen instructions: the
-// kernels that call it are bound by instruction fetch.
-template <bool DERIV>
-__device__ __forceinline__ void igamma_temme_sums(double eta, double r, double& S, double& Se, double& Sk) {
-  S = Se = Sk = 0.0;
-#pragma unroll 1
-  for (int k = fits::TEMME_K - 1; k >= 0; --k) {
-    const int lo = fits::TEMME_OFF[k], hi = fits::TEMME_OFF[k + 1];
-    double c = fits::TEMME_COEF[hi - 1], d = 0.0;
-#pragma unroll 1
-    for (int j = hi - 2; j >= lo; --j) {
-      if (DERIV) d = fma(d, eta, c);
-      c = fma(c, eta, fits::TEMME_COEF[j]);
-    }
-    S = fma(S, r, c);
-    if (DERIV) {
-      Se = fma(Se, r, d);
-      Sk = fma(Sk, r, (double)k * c);
-    }
-  }
-}
-
-// Out of line: one copy per kernel, fetched only by the warps that take it.
+// Out of line: one copy per kernel, fetched only by the warps that take it
+// (the kernels that call it are bound by instruction fetch, and its sums are
+// a few hundred straight-line FMAs).
 template <int ORDER>
 __device__ __noinline__ IgammaOut igamma_temme_d(double a, double x, const IgPre P) {
   IgammaOut o;
@@ -469,7 +446,7 @@ __device__ __noinline__ IgammaOut igamma_temme_d(double a, double x, const IgPre
   const double lm = log1pmx_d(u);  // ln(1+u) - u = -η²/2
   const double eta = u == 0.0 ? 0.0 : copysign(sqrt(-2.0 * lm), u);
   double S, Se, Sk;
-  igamma_temme_sums<(ORDER >= 1)>(eta, r, S, Se, Sk);
+  fits::temme_sums<(ORDER >= 1)>(eta, r, S, Se, Sk);
   const double pref = exp(fma(a, lm, -0.5 * (1.8378770664093453 + P.la())));  // e^(-aη²/2) / sqrt(2πa)
   const double s = eta * sqrt(0.5 * a);
   const double R = pref * S;
@@ -495,7 +472,12 @@ __device__ __noinline__ IgammaOut igamma_temme_d(double a, double x, const IgPre
 
 // FP64 evaluation.  ORDER 0: p,q; 1: + pa, px; 2: + paa, pax, pxx.
 // WANT_Q: Q is requested (selects the small-a formula for Q where it matters).
-template <int ORDER, bool WANT_Q = false>
+// UNIFORM: the uniform expansion takes its window (ORDER <= 1).  The callers
+// without per-row / per-column tables (the map kernel: independent points)
+// set it; the row-sorted sweep does not, because there the expansion's call
+// site alone measured slower for every element than the series it replaces
+// for the ~2% in its window (the sweep is bound by instruction fetch).
+template <int ORDER, bool WANT_Q = false, bool UNIFORM = false>
 __device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
   IgammaOut o;
   o.pa = o.px = o.paa = o.pax = o.pxx = 0.0;
@@ -519,7 +501,7 @@ __device__ inline IgammaOut igamma_eval_d(double a, double x, const IgPre& P) {
     o.q = 1.0;
     return o;
   }
-  if (ORDER <= 1 && igamma_temme_applies(a, x)) return igamma_temme_d<ORDER>(a, x, P);
+  if (UNIFORM && ORDER <= 1 && igamma_temme_applies(a, x)) return igamma_temme_d<ORDER>(a, x, P);
   const double lnD = igamma_log_prefix_d(a, x, P);
   const double lx = P.lx();
   // ∂P/∂x = x^(a-1) e^{-x} / Γ(a) = D·a/x
@@ -758,9 +740,9 @@ __device__ __forceinline__ bool igamma_needs_fp64_1(int region, float xf, const 
 
 // The FP64 evaluation with first derivatives as one out-of-line function,
 // for the mixed kernels' FP64 regions.
-template <bool WANT_Q>
+template <bool WANT_Q, bool UNIFORM>
 __device__ __noinline__ IgammaOut igamma_eval_d1_call(float a, float x, const IgPre P) {
-  return igamma_eval_d<1, WANT_Q>((double)a, (double)x, P);
+  return igamma_eval_d<1, WANT_Q, UNIFORM>((double)a, (double)x, P);
 }
 
 // Evaluation for float data.  P or Q alone (ORDER 0): FP32 in the light
@@ -769,21 +751,21 @@ __device__ __noinline__ IgammaOut igamma_eval_d1_call(float a, float x, const Ig
 // accumulation would exceed 1e-6) and the small-a Q.  First derivatives
 // (ORDER 1): FP32 in the regions of TSB_IG_FP32_MASK1 (igamma_eval_mf1), FP64
 // elsewhere.  Second derivatives: FP64.
-template <int ORDER, bool WANT_Q = false>
+template <int ORDER, bool WANT_Q = false, bool UNIFORM = false>
 __device__ inline IgammaOut igamma_eval_m(int region, float af, float xf, const IgPre& P) {
   if constexpr (ORDER >= 2) {
     return igamma_eval_d<ORDER, WANT_Q>((double)af, (double)xf, P);
   } else if constexpr (ORDER == 1) {
     // The FP64 evaluator is one out-of-line copy (igamma_eval_d1_call), so
     // the inline code is the FP32 path.
-    if (igamma_needs_fp64_1(region, xf, P, WANT_Q)) return igamma_eval_d1_call<WANT_Q>(af, xf, P);
+    if (igamma_needs_fp64_1(region, xf, P, WANT_Q)) return igamma_eval_d1_call<WANT_Q, UNIFORM>(af, xf, P);
     return igamma_eval_mf1<WANT_Q>(region, af, xf, P);
   } else {
     if (region == kIgSmallA || region == kIgSmallA0) {
-      if (WANT_Q) return igamma_eval_d<0, true>((double)af, (double)xf, P);
+      if (WANT_Q) return igamma_eval_d<0, true, UNIFORM>((double)af, (double)xf, P);
       region = kIgS1;
     }
-    if (!igamma_fp32_ok(region)) return igamma_eval_d<0, WANT_Q>((double)af, (double)xf, P);
+    if (!igamma_fp32_ok(region)) return igamma_eval_d<0, WANT_Q, UNIFORM>((double)af, (double)xf, P);
     return igamma_eval_mf<WANT_Q>(region, af, xf, P);
   }
 }
@@ -796,19 +778,21 @@ __device__ __forceinline__ IgammaOut igamma_saturated(bool upper_is_zero) {
   return o;
 }
 
-template <int ORDER, bool WANT_Q = false>
+template <int ORDER, bool WANT_Q = false, bool UNIFORM = false>
 __device__ __forceinline__ IgammaOut igamma_eval(int region, double a, double x, const IgPre& P) {
   if (region == kIgSat0 || region == kIgSat1) return igamma_saturated(region == kIgSat1);
-  return igamma_eval_d<ORDER, WANT_Q>(a, x, P);
+  return igamma_eval_d<ORDER, WANT_Q, UNIFORM>(a, x, P);
 }
-template <int ORDER, bool WANT_Q = false>
+template <int ORDER, bool WANT_Q = false, bool UNIFORM = false>
 __device__ __forceinline__ IgammaOut igamma_eval(int region, float a, float x, const IgPre& P) {
   if (region == kIgSat0 || region == kIgSat1) return igamma_saturated(region == kIgSat1);
-  return igamma_eval_m<ORDER, WANT_Q>(region, a, x, P);
+  return igamma_eval_m<ORDER, WANT_Q, UNIFORM>(region, a, x, P);
 }
+// Without tables (map-kernel callers of independent points): the uniform
+// expansion takes its window.
 template <int ORDER, bool WANT_Q = false, typename T>
 __device__ __forceinline__ IgammaOut igamma_eval(int region, T a, T x) {
-  return igamma_eval<ORDER, WANT_Q>(region, a, x, IgPre{nullptr, nullptr, (double)a, (double)x});
+  return igamma_eval<ORDER, WANT_Q, true>(region, a, x, IgPre{nullptr, nullptr, (double)a, (double)x});
 }
 
 }  // namespace tsb

@@ -48,16 +48,23 @@ struct IgammaAuxIO {
   }
 };
 
+// Each functor evaluates through eval_impl<UNIFORM>: the map kernel calls the
+// four-argument eval (independent points: the uniform expansion takes its
+// window), the kernels with per-row / per-column tables the six-argument one.
 template <typename T_, bool UPPER>
 struct IgammaFwd : IgammaAuxIO<0, 0, 1, T_> {
   using T = T_;
   static constexpr int NIN = 2, NOUT = 1, R = kIgRegions;
   static constexpr int MIN_BLOCKS = TSB_IGF_MINB;
   static constexpr bool REDUCE = false;
-  __device__ static void eval(int r, const T* in, T* out, uint32_t, const double* A = nullptr,
-                              const double* X = nullptr) {
-    const IgammaOut o = igamma_eval<0, UPPER>(r, in[0], in[1], IgammaFwd::pre(in, A, X));
+  template <bool UNIFORM>
+  __device__ static void eval_impl(int r, const T* in, T* out, const double* A, const double* X) {
+    const IgammaOut o = igamma_eval<0, UPPER, UNIFORM>(r, in[0], in[1], IgammaFwd::pre(in, A, X));
     out[0] = (T)(UPPER ? o.q : o.p);
+  }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t) { eval_impl<true>(r, in, out, nullptr, nullptr); }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t, const double* A, const double* X) {
+    eval_impl<false>(r, in, out, A, X);
   }
 };
 
@@ -69,8 +76,8 @@ struct IgammaBwd : IgammaAuxIO<1, 1, 2, T_> {
   // allocation (118 registers, 2 CTAs) on the 4096 x 4096 grid.
   static constexpr int MIN_BLOCKS = 4;
   static constexpr bool REDUCE = true;
-  __device__ static void eval(int r, const T* in, T* out, uint32_t mask, const double* A = nullptr,
-                              const double* X = nullptr) {
+  template <bool UNIFORM>
+  __device__ static void eval_impl(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
     const double sgn = UPPER ? -1.0 : 1.0;
     const double g = in[0];
     const IgPre P = IgammaBwd::pre(in, A, X);
@@ -79,9 +86,15 @@ struct IgammaBwd : IgammaAuxIO<1, 1, 2, T_> {
       out[1] = (T)(sgn * g * igamma_px_only((double)in[1], (double)in[2], P));
       return;
     }
-    const IgammaOut o = igamma_eval<1>(r, in[1], in[2], P);
+    const IgammaOut o = igamma_eval<1, false, UNIFORM>(r, in[1], in[2], P);
     out[0] = (T)(sgn * g * o.pa);
     out[1] = (T)(sgn * g * o.px);
+  }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t mask) {
+    eval_impl<true>(r, in, out, mask, nullptr, nullptr);
+  }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
+    eval_impl<false>(r, in, out, mask, A, X);
   }
   // Two-pass sweep of float data: pass 1 the FP32 elements, pass 2 the rest.
   static constexpr bool SPLIT = sizeof(T) == 4;
@@ -149,22 +162,28 @@ struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
   static constexpr int MIN_BLOCKS = 4;
   static constexpr int TILE_ROWS = TSB_IGFG_TR;
   static constexpr bool REDUCE = false;
-  __device__ static void eval(int r, const T* in, T* out, uint32_t mask, const double* A = nullptr,
-                              const double* X = nullptr) {
+  template <bool UNIFORM>
+  __device__ static void eval_impl(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
     const double sgn = UPPER ? -1.0 : 1.0;
     const IgPre P = IgammaFwdGrad::pre(in, A, X);
     // in[] are T: float data takes the mixed evaluators (igamma_eval_m)
     if (!(mask & 2u)) {
-      const IgammaOut o = igamma_eval<0, UPPER>(r, in[0], in[1], P);
+      const IgammaOut o = igamma_eval<0, UPPER, UNIFORM>(r, in[0], in[1], P);
       out[0] = (T)(UPPER ? o.q : o.p);
       out[1] = T(0);
       out[2] = (T)(sgn * igamma_px_only((double)in[0], (double)in[1], P));
       return;
     }
-    const IgammaOut o = igamma_eval<1, UPPER>(r, in[0], in[1], P);
+    const IgammaOut o = igamma_eval<1, UPPER, UNIFORM>(r, in[0], in[1], P);
     out[0] = (T)(UPPER ? o.q : o.p);
     out[1] = (T)(sgn * o.pa);
     out[2] = (T)(sgn * o.px);
+  }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t mask) {
+    eval_impl<true>(r, in, out, mask, nullptr, nullptr);
+  }
+  __device__ static void eval(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
+    eval_impl<false>(r, in, out, mask, A, X);
   }
   // Two-pass sweep of float data: pass 1 the FP32 elements (compact FP32
   // code alone in its kernel), pass 2 the rest in FP64.

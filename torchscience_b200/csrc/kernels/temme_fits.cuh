@@ -4,210 +4,316 @@
 namespace tsb {
 namespace fits {
 
-constexpr double TEMME_A_MIN = 20.0;
+constexpr double TEMME_A_MIN = 100.0;
 constexpr double TEMME_LAM_LO = 0.6;
 constexpr double TEMME_LAM_HI = 1.6;
-constexpr int TEMME_K = 12;
+constexpr int TEMME_K = 9;
 
-// c_k(η) = Σ_j TEMME_COEF[TEMME_OFF[k] + j] η^j, j < TEMME_OFF[k+1] - TEMME_OFF[k].
-__device__ const int TEMME_OFF[13] = {0, 23, 44, 63, 82, 100, 116, 131, 144, 155, 166, 175, 183};
-__device__ const double TEMME_COEF[183] = {
-    // c_0
-    -0.3333333333333333,
-    0.08333333333333333,
-    -0.014814814814814815,
-    0.0011574074074074073,
-    0.0003527336860670194,
-    -0.0001787551440329218,
-    3.919263178522438e-05,
-    -2.185448510679992e-06,
-    -1.85406221071516e-06,
-    8.296711340953087e-07,
-    -1.7665952736826078e-07,
-    6.707853543401498e-09,
-    1.0261809784240309e-08,
-    -4.382036018453353e-09,
-    9.14769958223679e-10,
-    -2.5514193994946248e-11,
-    -5.830772132550426e-11,
-    2.4361948020667415e-11,
-    -5.0276692801141755e-12,
-    1.1004392031956135e-13,
-    3.371763262400985e-13,
-    -1.392388722418162e-13,
-    2.8534893807047445e-14,
-    // c_1
-    -0.001851851851851852,
-    -0.003472222222222222,
-    0.0026455026455026454,
-    -0.0009902263374485596,
-    0.00020576131687242798,
-    -4.018775720164609e-07,
-    -1.8098550334489977e-05,
-    7.64916091608111e-06,
-    -1.6120900894563446e-06,
-    4.647127802807434e-09,
-    1.378633446915721e-07,
-    -5.752545603517705e-08,
-    1.1951628599778148e-08,
-    -1.7543241719747647e-11,
-    -1.0091543710600413e-09,
-    4.162792991842583e-10,
-    -8.56390702649298e-11,
-    6.067215101604758e-14,
-    7.1624989648114856e-12,
-    -2.933186643771437e-12,
-    5.996696365683689e-13,
-    // c_2
-    0.004133597883597883,
-    -0.0026813271604938273,
-    0.0007716049382716049,
-    2.0093878600823047e-06,
-    -0.0001073665322636516,
-    5.2923448829120125e-05,
-    -1.2760635188618728e-05,
-    3.423578734096138e-08,
-    1.3721957309062934e-06,
-    -6.298992138380055e-07,
-    1.4280614206064242e-07,
-    -2.0477098421990866e-10,
-    -1.409252991086752e-08,
-    6.228974084922022e-09,
-    -1.3670488396617114e-09,
-    9.428356159014678e-13,
-    1.2872252400089318e-10,
-    -5.5645956134363323e-11,
-    1.197593554636698e-11,
-    // c_3
-    0.0006494341563786008,
-    0.00022947209362139917,
-    -0.0004691894943952557,
-    0.00026772063206283885,
-    -7.561801671883977e-05,
-    -2.396505113867297e-07,
-    1.1082654115347302e-05,
-    -5.6749528269915965e-06,
-    1.4230900732435883e-06,
-    -2.7861080291528143e-11,
-    -1.6958404091930278e-07,
-    8.099464905388083e-08,
-    -1.9111168485973655e-08,
-    2.3928620439808118e-12,
-    2.0620131815488797e-09,
-    -9.460496661855133e-10,
-    2.1541049775774907e-10,
-    -1.388823336813903e-14,
-    -2.1894761681963938e-11,
-    // c_4
-    -0.0008618882909167117,
-    0.0007840392217200666,
-    -0.0002990724803031902,
-    -1.4638452578843418e-06,
-    6.641498215465122e-05,
-    -3.968365047179435e-05,
-    1.1375726970678419e-05,
-    2.507497226237533e-10,
-    -1.6954149536558305e-06,
-    8.907507532205309e-07,
-    -2.292934834000805e-07,
-    2.956794137544049e-11,
-    2.8865829742708783e-08,
-    -1.4189739437803219e-08,
-    3.4463580499464896e-09,
-    -2.3024517174528067e-13,
-    -3.9409233028046403e-10,
-    1.86023389685045e-10,
-    // c_5
-    -0.00033679855336635813,
-    -6.972813758365857e-05,
-    0.0002772753244959392,
-    -0.00019932570516188847,
-    6.797780477937208e-05,
-    1.419062920643967e-07,
-    -1.3594048189768693e-05,
-    8.018470256334202e-06,
-    -2.291481176508095e-06,
-    -3.252473551298454e-10,
-    3.4652846491085265e-07,
-    -1.8447187191171344e-07,
-    4.8240967037894184e-08,
-    -1.7989466721743514e-14,
-    -6.306194500013523e-09,
-    3.162417628774568e-09,
-    // c_6
-    0.0005313079364639922,
-    -0.0005921664373536939,
-    0.0002708782096718045,
-    7.902353232660328e-07,
-    -8.153969367561969e-05,
-    5.61168275310625e-05,
-    -1.8329116582843375e-05,
-    -3.0796134506033047e-09,
-    3.465155368803609e-06,
-    -2.0291327396058603e-06,
-    5.788792863149004e-07,
-    2.338630673826657e-13,
-    -8.828600746330484e-08,
-    4.7435958880408125e-08,
-    -1.2545415020710383e-08,
-    // c_7
-    0.00034436760689237765,
-    5.171790908260592e-05,
-    -0.00033493161081142234,
-    0.0002812695154763237,
-    -0.00010976582244684731,
-    -1.2741009095484485e-07,
-    2.7744451511563645e-05,
-    -1.8263488805711332e-05,
-    5.7876949497350525e-06,
-    4.93875893393627e-10,
-    -1.0595367014026043e-06,
-    6.166714376110408e-07,
-    -1.7562973359060463e-07,
-    // c_8
-    -0.0006526239185953094,
-    0.0008394987206720873,
-    -0.000438297098541721,
-    -6.969091458420552e-07,
-    0.00016644846642067547,
-    -0.00012783517679769218,
-    4.629953263691304e-05,
-    4.557909867922708e-09,
-    -1.0595271125805195e-05,
-    6.783342904865167e-06,
-    -2.1075476666258803e-06,
-    // c_9
-    -0.0005967612901927463,
-    -7.204895416020011e-05,
-    0.0006782308837667328,
-    -0.0006401475260262758,
-    0.00027750107634328704,
-    1.819700838046515e-07,
-    -8.479507117068503e-05,
-    6.105192082501531e-05,
-    -2.1073920183404862e-05,
-    -8.858589014125599e-10,
-    4.5284535953805374e-06,
-    // c_10
-    0.0013324454494800656,
-    -0.0019144384985654776,
-    0.0011089369134596636,
-    9.9324041226423e-07,
-    -0.0005087450129309319,
-    0.00042735056665392886,
-    -0.00016858853767910798,
-    -8.1301893922785e-09,
-    4.5284402370562144e-05,
-    // c_11
-    0.001579727660730835,
-    0.00016251626278391583,
-    -0.0020633421035543276,
-    0.00213896861856891,
-    -0.0010108559391263003,
-    -3.99127055299192e-07,
-    0.0003623502508476469,
-    -0.00028143901463712157,
-};
+// S = Σ_k c_k(η) r^k with r = 1/a; when DERIV also Se = Σ_k c_k'(η) r^k and
+// Sk = Σ_k k c_k(η) r^k (so that ∂S/∂a = -r Sk).  Horner in η for each c_k (and its
+// derivative), then in r, written out with the coefficients as constants: the
+// evaluation is its FMAs alone, about two per coefficient.
+template <bool DERIV>
+__device__ __forceinline__ void temme_sums(double eta, double r, double& S, double& Se, double& Sk) {
+  double c, d;
+  S = Se = Sk = 0.0;
+  // c_8: 3 terms
+  c = -0.000438297098541721;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0008394987206720873);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0006526239185953094);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = fma(Sk, r, 8.0 * c);
+  }
+  // c_7: 5 terms
+  c = -0.00010976582244684731;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0002812695154763237);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.00033493161081142234);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 5.171790908260592e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.00034436760689237765);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = fma(Sk, r, 7.0 * c);
+  }
+  // c_6: 9 terms
+  c = 3.465155368803609e-06;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -3.0796134506033047e-09);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.8329116582843375e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 5.61168275310625e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -8.153969367561969e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 7.902353232660328e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0002708782096718045);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0005921664373536939);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0005313079364639922);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = fma(Sk, r, 6.0 * c);
+  }
+  // c_5: 12 terms
+  c = -1.8447187191171344e-07;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 3.4652846491085265e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -3.252473551298454e-10);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -2.291481176508095e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 8.018470256334202e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.3594048189768693e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.419062920643967e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 6.797780477937208e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.00019932570516188847);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0002772753244959392);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -6.972813758365857e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.00033679855336635813);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = fma(Sk, r, 5.0 * c);
+  }
+  // c_4: 14 terms
+  c = -1.4189739437803219e-08;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 2.8865829742708783e-08);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 2.956794137544049e-11);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -2.292934834000805e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 8.907507532205309e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.6954149536558305e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 2.507497226237533e-10);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.1375726970678419e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -3.968365047179435e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 6.641498215465122e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.4638452578843418e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0002990724803031902);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0007840392217200666);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0008618882909167117);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = fma(Sk, r, 4.0 * c);
+  }
+  // c_3: 16 terms
+  c = -9.460496661855133e-10;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 2.0620131815488797e-09);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 2.3928620439808118e-12);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.9111168485973655e-08);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 8.099464905388083e-08);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.6958404091930278e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -2.7861080291528143e-11);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.4230900732435883e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -5.6749528269915965e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.1082654115347302e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -2.396505113867297e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -7.561801671883977e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.00026772063206283885);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0004691894943952557);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.00022947209362139917);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0006494341563786008);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = fma(Sk, r, 3.0 * c);
+  }
+  // c_2: 18 terms
+  c = -5.5645956134363323e-11;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.2872252400089318e-10);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 9.428356159014678e-13);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.3670488396617114e-09);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 6.228974084922022e-09);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.409252991086752e-08);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -2.0477098421990866e-10);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.4280614206064242e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -6.298992138380055e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.3721957309062934e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 3.423578734096138e-08);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.2760635188618728e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 5.2923448829120125e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0001073665322636516);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 2.0093878600823047e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0007716049382716049);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0026813271604938273);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.004133597883597883);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = fma(Sk, r, 2.0 * c);
+  }
+  // c_1: 21 terms
+  c = 5.996696365683689e-13;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -2.933186643771437e-12);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 7.1624989648114856e-12);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 6.067215101604758e-14);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -8.56390702649298e-11);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 4.162792991842583e-10);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.0091543710600413e-09);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.7543241719747647e-11);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.1951628599778148e-08);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -5.752545603517705e-08);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.378633446915721e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 4.647127802807434e-09);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.6120900894563446e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 7.64916091608111e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.8098550334489977e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -4.018775720164609e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.00020576131687242798);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0009902263374485596);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0026455026455026454);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.003472222222222222);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.001851851851851852);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = fma(Sk, r, 1.0 * c);
+  }
+  // c_0: 23 terms
+  c = 2.8534893807047445e-14;
+  d = 0.0;
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.392388722418162e-13);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 3.371763262400985e-13);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.1004392031956135e-13);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -5.0276692801141755e-12);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 2.4361948020667415e-11);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -5.830772132550426e-11);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -2.5514193994946248e-11);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 9.14769958223679e-10);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -4.382036018453353e-09);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 1.0261809784240309e-08);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 6.707853543401498e-09);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.7665952736826078e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 8.296711340953087e-07);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -1.85406221071516e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -2.185448510679992e-06);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 3.919263178522438e-05);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.0001787551440329218);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0003527336860670194);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.0011574074074074073);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.014814814814814815);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, 0.08333333333333333);
+  if (DERIV) d = fma(d, eta, c);
+  c = fma(c, eta, -0.3333333333333333);
+  S = fma(S, r, c);
+  if (DERIV) {
+    Se = fma(Se, r, d);
+    Sk = Sk * r;
+  }
+}
 
 }  // namespace fits
 }  // namespace tsb
