@@ -78,8 +78,8 @@ ELEMS = ROWS * COLS + STRESS
 # From one ncu capture of the dominant kernel (sweep2d_kernel<IgammaFwdGrad<double>, double>, one launch on
 # this grid, the current kernel): dram__bytes_read.sum + dram__bytes_write.sum, and the FP64 pipe's active
 # fraction (sm__pipe_fp64_cycles_active.avg.pct_of_peak_sustained_active).
-TRAFFIC_BYTES_P_FWDGRAD = 385.74e6
-PIPE_FRAC_FP64 = 0.304
+TRAFFIC_BYTES_P_FWDGRAD = 386.81e6
+PIPE_FRAC_FP64 = 0.378
 TRAFFIC_SOURCE = ("ncu --set full --clock-control none -k regex:'sweep2d_kernel|stream2d_kernel' -c 4 over one "
                   "FP64 and one float32 step of this workload; the first captured launch (the FP64 fused forward)")
 

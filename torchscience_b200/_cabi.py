@@ -86,11 +86,13 @@ def call(name: str, inputs, outputs, precision: int = 0, workspace: torch.Tensor
 
 def sweep_scratch_bytes(shape) -> int:
     """Bytes of the workspace that only the row-sorted sweep of a 2-D grid
-    uses (its row order, row and column tables of 16 doubles per entry, and
-    task counter): the last part of what tsb_workspace_bytes asks for on such
-    a grid."""
+    uses (its row order, row and column tables of 16 doubles per entry, one
+    32-bit column mask per 32 x 32 task, and the task counters): the last part
+    of what tsb_workspace_bytes asks for on such a grid."""
     n0, n1 = (shape[-2], shape[-1]) if len(shape) >= 2 else (0, 0)
-    return ((max(n0, n1) * 4 + 255) & ~255) + (((n0 + n1) * 16 * 8 + 255) & ~255) + 256
+    tasks = ((n0 + 31) // 32) * ((n1 + 31) // 32)
+    return (((max(n0, n1) * 4 + 255) & ~255) + (((n0 + n1) * 16 * 8 + 255) & ~255) + ((tasks * 4 + 255) & ~255)
+            + 256)
 
 
 def run(name: str, *inputs, n_out: int = 1, precision: int = 0, out_shapes=None, sweep: bool = True) -> list[torch.Tensor]:
