@@ -184,6 +184,35 @@ def max_over_ranks(values, dist, device):
     return t.tolist()
 
 
+def host_link_rate(host_buf, dev) -> float:
+    """GB/s each way of the host link with both directions busy: a copy of
+    host_buf (pinned) to the device on one stream while the device copy goes
+    back to another pinned buffer on a second stream, best of 3 after one
+    warm-up (CUDA events)."""
+    d_in = torch.empty(host_buf.shape, dtype=host_buf.dtype, device=dev)
+    d_out = torch.empty_like(d_in)
+    back = torch.empty_like(host_buf).pin_memory()
+    s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    best = float("inf")
+    for i in range(4):
+        main = torch.cuda.current_stream(dev)
+        s1.wait_stream(main)
+        s2.wait_stream(main)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        with torch.cuda.stream(s1):
+            d_in.copy_(host_buf, non_blocking=True)
+        with torch.cuda.stream(s2):
+            back.copy_(d_out, non_blocking=True)
+        main.wait_stream(s1)
+        main.wait_stream(s2)
+        e1.record()
+        e1.synchronize()
+        if i:
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+    return host_buf.numel() * host_buf.element_size() / best / 1e9
+
+
 def count_launches(fn) -> int:
     """Kernels this library launches in one call of fn, read from the
     library's own launch counter (tsb_launch_count)."""
@@ -477,6 +506,7 @@ def our_arm(args):
         main.wait_stream(s_out)
 
     t_e2e = timed_steps(e2e_step, args.steps, 2, flush)
+    link = host_link_rate(y_host, dev)
     torch.cuda.synchronize()
     # the pipelined results against the device step's (same kernels, so the
     # values and grad_a agree exactly; grad_x is summed in another order)
@@ -551,6 +581,10 @@ def our_arm(args):
             # (134 MB each on the grid) bound the end-to-end step, the kernels overlapping them
             "h2d_gb_s": h2d / (t_e2e / args.steps) / 1e9,
             "d2h_gb_s": d2h / (t_e2e / args.steps) / 1e9,
+            # the same byte count copied both ways at once with nothing else running: the step's bound
+            "host_link_gb_s_each_way": link,
+            "link_bound_gelem_s": total / args.steps / (max(h2d, d2h) / (link * 1e9)) / 1e9,
+            "frac_of_link_bound": (max(h2d, d2h) / (link * 1e9)) / (t_e2e / args.steps),
         },
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),

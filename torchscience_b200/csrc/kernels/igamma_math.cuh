@@ -73,18 +73,25 @@ enum IgammaAuxA : int {
   kIgA_RA,      // 1/a
   kIgA_PSI,     // ψ(a)  (first and second derivatives)
   kIgA_PSI1,    // ψ'(a) (second derivatives)
-  kIgA_LGF,     // lgammaf(a+1) in float (classification)
-  kIgA_LAF,     // __logf(a)
-  kIgA_LA1F,    // __logf(a+1)
-  kIgA_PRFF,    // ψ(a) + 1/a as a packed float-float pair (the mixed kernels' routing test)
+  kIgA_F1,      // two floats in one slot: lgammaf(a+1) | __logf(a)      (classification)
+  kIgA_F2,      // two floats in one slot: __logf(a+1) | float(ψ(a)+1/a) (classification, mixed routing)
   kIgAuxA
 };
 enum IgammaAuxX : int {
   kIgX_LX = 0,  // ln x
   kIgX_RX,      // 1/x
-  kIgX_LXF,     // __logf(x)
+  kIgX_F1,      // __logf(x) in the slot's high half
   kIgAuxX
 };
+
+// The float table entries are packed two to a double slot and read as the
+// slot's 32-bit halves, which costs no conversion instruction (a float
+// stored as a double would be converted back on every element).
+__device__ __forceinline__ double f2_pack(float hi, float lo) {
+  return __hiloint2double(__float_as_int(hi), __float_as_int(lo));
+}
+__device__ __forceinline__ float f2_hi(double d) { return __int_as_float(__double2hiint(d)); }
+__device__ __forceinline__ float f2_lo(double d) { return __int_as_float(__double2loint(d)); }
 
 // A double split into floats hi + lo (|lo| <= ulp(hi)/2), for the mixed
 // kernels' exponentials: ln D = a ln x - x - lnΓ(a+1) cancels by up to ~1e4
@@ -96,14 +103,6 @@ struct IgFF {
 __device__ __forceinline__ IgFF ff_split(double v) {
   const float hi = (float)v;
   return IgFF{hi, (float)(v - (double)hi)};
-}
-__device__ __forceinline__ double ff_pack(double v) {
-  const IgFF f = ff_split(v);
-  return __longlong_as_double(((long long)__float_as_int(f.hi) << 32) | (unsigned int)__float_as_int(f.lo));
-}
-__device__ __forceinline__ IgFF ff_unpack(double d) {
-  const long long b = __double_as_longlong(d);
-  return IgFF{__int_as_float((int)(b >> 32)), __int_as_float((int)(b & 0xffffffffll))};
 }
 // exp(hi + lo) = exp(hi) (1 + lo) for |lo| << 1.
 __device__ __forceinline__ float ff_exp(IgFF x) { return expf(x.hi) * (1.0f + x.lo); }
@@ -120,15 +119,13 @@ __device__ inline void igamma_aux_a(double a, double* o) {
   o[kIgA_RA] = 1.0 / a;
   o[kIgA_PSI] = ORDER >= 1 ? digamma_d(a) : 0.0;
   o[kIgA_PSI1] = ORDER >= 2 ? trigamma_d(a) : 0.0;
-  o[kIgA_LGF] = lgammaf(af + 1.0f);
-  o[kIgA_LAF] = __logf(af);
-  o[kIgA_LA1F] = __logf(af + 1.0f);
-  o[kIgA_PRFF] = ff_pack(o[kIgA_PSI] + o[kIgA_RA]);
+  o[kIgA_F1] = f2_pack(lgammaf(af + 1.0f), __logf(af));
+  o[kIgA_F2] = f2_pack(__logf(af + 1.0f), (float)(o[kIgA_PSI] + o[kIgA_RA]));
 }
 __device__ inline void igamma_aux_x(double x, double* o) {
   o[kIgX_LX] = log(x);
   o[kIgX_RX] = 1.0 / x;
-  o[kIgX_LXF] = __logf((float)x);
+  o[kIgX_F1] = f2_pack(__logf((float)x), 0.0f);
 }
 
 struct IgPre {
@@ -140,13 +137,13 @@ struct IgPre {
   __device__ double ra() const { return A ? A[kIgA_RA] : 1.0 / a; }
   __device__ double psi() const { return A ? A[kIgA_PSI] : digamma_d(a); }
   __device__ double psi1() const { return A ? A[kIgA_PSI1] : trigamma_d(a); }
-  __device__ float lgf() const { return A ? (float)A[kIgA_LGF] : lgammaf((float)a + 1.0f); }
-  __device__ float laf() const { return A ? (float)A[kIgA_LAF] : __logf((float)a); }
-  __device__ float la1f() const { return A ? (float)A[kIgA_LA1F] : __logf((float)a + 1.0f); }
+  __device__ float lgf() const { return A ? f2_hi(A[kIgA_F1]) : lgammaf((float)a + 1.0f); }
+  __device__ float laf() const { return A ? f2_lo(A[kIgA_F1]) : __logf((float)a); }
+  __device__ float la1f() const { return A ? f2_hi(A[kIgA_F2]) : __logf((float)a + 1.0f); }
   __device__ double lx() const { return X ? X[kIgX_LX] : log(x); }
-  __device__ IgFF prff() const { return A ? ff_unpack(A[kIgA_PRFF]) : ff_split(digamma_d(a) + 1.0 / a); }
+  __device__ float prf() const { return A ? f2_lo(A[kIgA_F2]) : (float)(digamma_d(a) + 1.0 / a); }
   __device__ double rx() const { return X ? X[kIgX_RX] : 1.0 / x; }
-  __device__ float lxf() const { return X ? (float)X[kIgX_LXF] : __logf((float)x); }
+  __device__ float lxf() const { return X ? f2_hi(X[kIgX_F1]) : __logf((float)x); }
 };
 
 // ln D(a,x), D = x^a e^{-x} / Γ(a+1).
@@ -735,7 +732,7 @@ __device__ inline IgammaOut igamma_eval_mf1(int region, float a, float x, const 
 __device__ __forceinline__ bool igamma_needs_fp64_1(int region, float xf, const IgPre& P, bool want_q) {
   return region == kIgSpecial || !((TSB_IG_FP32_MASK1 >> region) & 1u) ||
          (want_q && (region == kIgSmallA || region == kIgSmallA0)) ||
-         (region == kIgSmallA && P.lxf() > P.prff().hi) || ((region == kIgC0 || region == kIgC00) && !(xf >= 20.0f));
+         (region == kIgSmallA && P.lxf() > P.prf()) || ((region == kIgC0 || region == kIgC00) && !(xf >= 20.0f));
 }
 
 // The FP64 evaluation with first derivatives as one out-of-line function,
