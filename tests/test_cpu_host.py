@@ -118,7 +118,7 @@ def test_meta_broadcast_and_promotion():
 def test_integer_and_complex_inputs_raise_not_implemented():
     with pytest.raises(NotImplementedError, match="Long"):
         sf.log_gamma(torch.empty(3, dtype=torch.long, device="meta"))
-    # complex dtypes: the gamma family has kernels; the other operators raise
+    # complex dtypes: the gamma and beta families have kernels; the other operators raise
     with pytest.raises(NotImplementedError, match="complex dtypes"):
         sf.bessel_j_0(torch.empty(3, dtype=torch.complex64, device="meta"))
     for fn in (sf.log_gamma, sf.gamma, sf.digamma, sf.trigamma):

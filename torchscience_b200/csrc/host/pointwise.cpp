@@ -28,7 +28,7 @@ int32_t to_tsb_dtype(at::ScalarType t) {
 // Operators with complex64 / complex128 kernels (and their backward and
 // double-backward ops).
 bool takes_complex(const char* name) {
-  static const char* const ops[] = {"log_gamma", "gamma", "digamma", "trigamma"};
+  static const char* const ops[] = {"log_gamma", "gamma", "digamma", "trigamma", "log_beta", "beta"};
   const std::string n(name);
   for (const char* op : ops) {
     const std::string o(op);
@@ -87,7 +87,7 @@ at::ScalarType checked_common_dtype(const char* name, at::TensorList inputs) {
   const at::ScalarType dt = at::native::result_type(state);
   if (at::isComplexType(dt)) {
     TORCH_CHECK_NOT_IMPLEMENTED(takes_complex(name), "\"", name, "\" not implemented for '", c10::toString(dt),
-                                "' in torchscience_b200 (complex dtypes: log_gamma, gamma, digamma, trigamma)");
+                                "' in torchscience_b200 (complex dtypes: log_gamma, gamma, digamma, trigamma, log_beta, beta)");
     TORCH_CHECK_NOT_IMPLEMENTED(dt == at::kComplexFloat || dt == at::kComplexDouble, "\"", name,
                                 "\" not implemented for '", c10::toString(dt), "'");
     return dt;
@@ -215,9 +215,13 @@ std::vector<at::Tensor> run_reduced(OpFn fn, const char* name, at::TensorList al
   std::vector<tsb_tensor> din, dout;
   for (const auto& t : ins) din.push_back(describe(t, full));
   for (int i = 0; i < n_fwd; ++i) dout.push_back(want[i] ? describe(grads[i], full) : describe(at::Tensor(), full, false));
-  const int64_t ws = tsb_workspace_bytes(din.data(), (int32_t)din.size(), dout.data(), (int32_t)dout.size());
+  // Complex entry points do not reduce outputs: their broadcast gradients
+  // take the full-shape path below.
+  const int64_t ws = at::isComplexType(dt) ? (int64_t)TSB_ERR_LAYOUT
+                                           : tsb_workspace_bytes(din.data(), (int32_t)din.size(), dout.data(),
+                                                                 (int32_t)dout.size());
   if (ws == TSB_ERR_LAYOUT) {
-    // Not a 2-D broadcast pattern: full-shape gradients + sum_to.
+    // Not a 2-D broadcast pattern (or complex data): full-shape gradients + sum_to.
     std::vector<at::Tensor> full_grads(n_fwd);
     std::vector<tsb_tensor> dfull;
     for (int i = 0; i < n_fwd; ++i) {

@@ -146,3 +146,79 @@ struct PolygammaBwdBwd {  // in = {gg_n, gg_z, grad, n, z}
 };
 
 }  // namespace tsb
+
+// ------------------------------------------------------------ complex data
+// log_beta and beta of complex64 / complex128 arguments (evaluated in
+// complex128): ln B(a, b) = lnΓ(a) + lnΓ(b) - lnΓ(a+b) with the principal
+// lnΓ (log_beta.h:15-17 takes the same sum of its complex log_gamma), and
+// B = exp(ln B) (beta.h:13-15).  Gradients follow the gamma family's
+// convention (PyTorch's conjugate Wirtinger gradients): for f(a, b)
+// holomorphic in each argument, backward = (g·conj(f_a), g·conj(f_b)) and the
+// double backward = (gg_a·f_a + gg_b·f_b,
+//   conj(gg_a)·g·conj(f_aa) + conj(gg_b)·g·conj(f_ab),
+//   conj(gg_a)·g·conj(f_ab) + conj(gg_b)·g·conj(f_bb)),
+// with f_a = ψ(a) - ψ(a+b), f_aa = ψ'(a) - ψ'(a+b), f_ab = -ψ'(a+b) for
+// ln B, and B times the logarithmic derivatives for B.  (The reference's
+// complex log_beta_backward.h:19-27 does not conjugate.)
+#include "complex_gamma.cuh"
+
+namespace tsb {
+
+struct CBetaDerivs {
+  cdouble f, fa, fb, faa, fab, fbb;
+};
+template <bool EXP, int ORDER>
+__device__ inline CBetaDerivs cbeta_derivs(cdouble a, cdouble b) {
+  CBetaDerivs d;
+  const cdouble s = a + b;
+  const cdouble lb = loggamma_c(a) + loggamma_c(b) - loggamma_c(s);
+  d.f = EXP ? cuda::std::exp(lb) : lb;
+  d.fa = d.fb = d.faa = d.fab = d.fbb = cdouble(0.0, 0.0);
+  if (ORDER >= 1) {
+    const cdouble ps = digamma_c(s), da = digamma_c(a) - ps, db = digamma_c(b) - ps;
+    d.fa = EXP ? d.f * da : da;
+    d.fb = EXP ? d.f * db : db;
+    if (ORDER >= 2) {
+      const cdouble p1 = trigamma_c(s), daa = trigamma_c(a) - p1, dbb = trigamma_c(b) - p1, dab = -p1;
+      d.faa = EXP ? d.f * (da * da + daa) : daa;
+      d.fab = EXP ? d.f * (da * db + dab) : dab;
+      d.fbb = EXP ? d.f * (db * db + dbb) : dbb;
+    }
+  }
+  return d;
+}
+
+template <bool EXP>
+struct CBetaFwd {  // in = {a, b}
+  using T = cdouble;
+  static constexpr int NIN = 2, NOUT = 1, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) { out[0] = cbeta_derivs<EXP, 0>(in[0], in[1]).f; }
+};
+template <bool EXP>
+struct CBetaBwd {  // in = {grad, a, b}, out = {grad_a, grad_b}
+  using T = cdouble;
+  static constexpr int NIN = 3, NOUT = 2, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const CBetaDerivs d = cbeta_derivs<EXP, 1>(in[1], in[2]);
+    out[0] = in[0] * cuda::std::conj(d.fa);
+    out[1] = in[0] * cuda::std::conj(d.fb);
+  }
+};
+template <bool EXP>
+struct CBetaBwdBwd {  // in = {gg_a, gg_b, grad, a, b}, out = {grad_grad_output, grad_a, grad_b}
+  using T = cdouble;
+  static constexpr int NIN = 5, NOUT = 3, R = 1;
+  static constexpr bool REDUCE = false;
+  __device__ static void eval(int, const T* in, T* out, uint32_t) {
+    const cdouble gga = in[0], ggb = in[1], g = in[2];
+    const CBetaDerivs d = cbeta_derivs<EXP, 2>(in[3], in[4]);
+    const cdouble cga = cuda::std::conj(gga), cgb = cuda::std::conj(ggb);
+    out[0] = gga * d.fa + ggb * d.fb;
+    out[1] = g * (cga * cuda::std::conj(d.faa) + cgb * cuda::std::conj(d.fab));
+    out[2] = g * (cga * cuda::std::conj(d.fab) + cgb * cuda::std::conj(d.fbb));
+  }
+};
+
+}  // namespace tsb
