@@ -538,6 +538,37 @@ static __device__ __noinline__ H2f1Grad h2f1_grad(double a, double b, double c, 
   return g;
 }
 
+// The two halves of h2f1_grad for the map kernel's rescue list.  The first
+// returns false (g untouched) where h2f1_grad would fall back from the
+// connection formula to the evaluator search; the second is that fallback
+// alone.  Together they give h2f1_grad's results bit for bit, but the
+// declined elements run their long series in full warps.
+static __device__ __noinline__ bool h2f1_grad_first(double a, double b, double c, double z, double eps,
+                                                    H2f1Grad& g) {
+  double sv;
+  if (h2f1_special(a, b, c, z, sv, eps)) {
+    g.v = sv;
+    g.dz = h2f1_dz(a, b, c, z, eps);
+    h2f1_fd_grad(a, b, c, z, g, eps);
+    return true;
+  }
+  const int region = h2f1_region_of(z);
+  const H2Plan P = h2f1_plan(region, a, b, c, z);
+  if (P.method == kH2mSeries) {
+    g = h2f1_grad(a, b, c, z, eps);
+    return true;
+  }
+  const H2Val G = h2f1_connect<true>(P.p, P.q, c, 1.0 - P.x);
+  if (!(G.err <= 64.0 * kH2Ulp * fabs(G.v))) return false;
+  g = h2f1_assemble(P, G, z);
+  return true;
+}
+static __device__ __noinline__ H2f1Grad h2f1_grad_fallback(double a, double b, double c, double z) {
+  H2Plan P;
+  h2f1_eval(h2f1_region_of(z), a, b, c, z, &P);
+  return h2f1_assemble(P, h2f1_core<true>(P.method, P.p, P.q, c, P.x), z);
+}
+
 // Hessian of F in (a, b, c, z), symmetric, packed as
 // [aa, ab, ac, az, bb, bc, bz, cc, cz, zz], with the gradient.
 struct H2f1Hess {

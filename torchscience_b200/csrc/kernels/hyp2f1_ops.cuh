@@ -4,7 +4,13 @@
 // hypergeometric_2_f_1_backward_backward.h:12-125 (gg_out, then the new
 // grads in argument order).  Every precision evaluates in FP64 (the
 // connection formulas cancel by up to ~1e3 on the benchmark domain, beyond
-// what an FP32 bulk can absorb at 1e-6) and stores in the data type.
+// what an FP32 bulk can absorb at 1e-6) and stores in the data type.  The
+// backward declines the elements whose connection formula cancels (the
+// evaluator search and its long direct series with derivatives) to the map
+// kernel's rescue list, which evaluates them in full warps after the tile:
+// 1.7x on the benchmark's fwd + grads.  The forward keeps them in place: its
+// declined elements would evaluate the connection formula twice, which
+// measured 35% slower.
 #pragma once
 
 #include "dispatch.cuh"
@@ -62,11 +68,29 @@ struct Hyp2f1Bwd {
       out[3] = (T)(g * h2f1_dz(a, b, c, z, h2f1_eps_for<T>()));
       return;
     }
-    const H2f1Grad d = h2f1_grad(a, b, c, z, h2f1_eps_for<T>());
+    store(g, h2f1_grad(a, b, c, z, h2f1_eps_for<T>()), out);
+  }
+  __device__ static void store(double g, const H2f1Grad& d, T* out) {
     out[0] = (T)(g * d.da);
     out[1] = (T)(g * d.db);
     out[2] = (T)(g * d.dc);
     out[3] = (T)(g * d.dz);
+  }
+  // Elements whose connection formula cancels go through the rescue list.
+  static constexpr bool RESCUE = true;
+  __device__ static bool eval_first(int r, const T* in, T* out, uint32_t mask) {
+    if (!(mask & 7u)) {
+      eval(r, in, out, mask);
+      return true;
+    }
+    H2f1Grad d;
+    if (!h2f1_grad_first((double)in[1], (double)in[2], (double)in[3], (double)in[4], h2f1_eps_for<T>(), d))
+      return false;
+    store((double)in[0], d, out);
+    return true;
+  }
+  __device__ static void eval_rescue(int, const T* in, T* out, uint32_t) {
+    store((double)in[0], h2f1_grad_fallback((double)in[1], (double)in[2], (double)in[3], (double)in[4]), out);
   }
 };
 
