@@ -76,30 +76,44 @@ __device__ inline IbetaCF ibeta_cf(double p, double q, double y, double sp, doub
       Ap1 = Ap, Bp1 = Bp, Aq1 = Aq, Bq1 = Bq;
     }
     A2 = A1, B2 = B1, A1 = A, B1 = B;
-    double s = 1.0 / (fabs(B) > 1e-300 ? B : 1e-300);
-    A1 *= s, A2 *= s, B1 *= s, B2 *= s;
-    if (DERIVS) Ap1 *= s, Ap2 *= s, Bp1 *= s, Bp2 *= s, Aq1 *= s, Aq2 *= s, Bq1 *= s, Bq2 *= s;
   };
+  // The d_n and their p- and q-derivatives share reciprocals (two for an
+  // odd term, one for an even one; products kept apart so that no
+  // intermediate overflows before the parameters do), and the recurrences
+  // are rescaled by 1/B_n once per pair of terms, after which B_n = 1 and
+  // K = A_n.  Two terms grow the recurrences by at most (1 + |d|)^2 with
+  // |d| below about (p + q) / p, inside the exponent range for parameters
+  // below 1e150.
   {  // counted loop: reaching the cap is recorded (note_unconverged)
     int m = 0;
     for (; m < ib::kMaxPairs; ++m) {
       const double md = m;
-      {  // d_(2m+1)
+      {  // d_(2m+1) = -u v y / (w w1); ∂p ln d = 1/u + 1/v - 1/w - 1/w1, ∂q ln d = 1/v
         const double u = p + md, v = pq + md, w = p + 2.0 * md, w1 = w + 1.0;
-        const double d = -(u * v * y) / (w * w1);
-        const double dp = d * ((1.0 / u + 1.0 / v) - (1.0 / w + 1.0 / w1));
-        step(d, DERIVS ? dp : 0.0, DERIVS ? d / v : 0.0);
+        const double uv = u * v, ww = w * w1;
+        if (DERIVS) {
+          const double ruv = 1.0 / uv, rww = 1.0 / ww;
+          const double d = -(uv * y) * rww;
+          step(d, d * ((u + v) * ruv - (w + w1) * rww), d * (u * ruv));
+        } else {
+          step(-(uv * y) / ww, 0.0, 0.0);
+        }
       }
-      {  // d_(2m+2)
+      {  // d_(2m+2) = (q - k) k y / (w w1); ∂p ln d = -1/w - 1/w1, ∂q d = k y / (w w1)
         const double k = md + 1.0, w = p + 2.0 * md + 1.0, w1 = w + 1.0;
-        const double r = k * y / (w * w1);
+        const double rho = 1.0 / (w * w1);
+        const double r = k * y * rho;
         const double d = (q - k) * r;
-        step(d, DERIVS ? -d * (1.0 / w + 1.0 / w1) : 0.0, r);
+        step(d, DERIVS ? -d * ((w + w1) * rho) : 0.0, r);
       }
-      const double Kn = A1 / B1;
+      const double s = 1.0 / (fabs(B1) > 1e-300 ? B1 : 1e-300);
+      A1 *= s, A2 *= s, B2 *= s;
+      B1 = 1.0;
+      if (DERIVS) Ap1 *= s, Ap2 *= s, Bp1 *= s, Bp2 *= s, Aq1 *= s, Aq2 *= s, Bq1 *= s, Bq2 *= s;
+      const double Kn = A1;
       bool done = fabs(Kn - K) <= ib::kTol * fabs(Kn);
       if (DERIVS) {
-        const double Kpn = (Ap1 - Kn * Bp1) / B1, Kqn = (Aq1 - Kn * Bq1) / B1;
+        const double Kpn = fma(-Kn, Bp1, Ap1), Kqn = fma(-Kn, Bq1, Aq1);
         done = done && fabs(Kpn - Kp) <= ib::kTolD * (fabs(Kpn) + fabs(Kn) * sp) &&
                fabs(Kqn - Kq) <= ib::kTolD * (fabs(Kqn) + fabs(Kn) * sq);
         Kp = Kpn, Kq = Kqn;
