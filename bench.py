@@ -428,20 +428,27 @@ def our_arm(args):
 
     # The step runs in row chunks on three streams, so that copying the
     # upstream gradient in, evaluating and copying results out overlap (PCIe
-    # is full duplex).  The forwards need only a and x, so they all run first
-    # and their outputs start back to the host while g is still arriving; each
-    # chunk's backward runs as its slice of g lands.  Every chunk goes through
-    # the public API (special_functions + torch.autograd.grad); grad_x is the
-    # sum of the chunks' reduced gradients, then (several ranks) of the ranks'.
+    # is full duplex).  a and x go in first, so the grid's forwards start at
+    # once and their outputs start back to the host while the rest arrives;
+    # the stress points and their gradient go in next and are evaluated
+    # (forward and backward) behind the grid's forwards, so their results
+    # travel back early too; then g arrives chunk by chunk, each chunk's
+    # backward running as its slice lands.  What is left after the last
+    # byte of g is one chunk's backward and two 32 KB gradients.  Every chunk
+    # goes through the public API (special_functions + torch.autograd.grad);
+    # grad_x is the sum of the chunks' reduced gradients, then (several
+    # ranks) of the ranks'.
     from torchscience_b200.shard import row_range, sum_over_ranks
 
     chunks = 8
     bounds = [row_range(rows_local, i, chunks) for i in range(chunks)]
     s_in, s_comp, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     g_dev = torch.empty(rows_local, COLS, dtype=torch.float64, device=dev)
-    ev_in = [torch.cuda.Event() for _ in range(chunks + 2)]
-    ev_y = [torch.cuda.Event() for _ in range(chunks + 1)]
-    ev_out = [torch.cuda.Event() for _ in range(chunks + 1)]
+    ev_g = [torch.cuda.Event() for _ in range(chunks)]
+    ev_ax, ev_stress_in = torch.cuda.Event(), torch.cuda.Event()
+    ev_y = [torch.cuda.Event() for _ in range(chunks)]
+    ev_ga = [torch.cuda.Event() for _ in range(chunks)]
+    ev_stress_out = torch.cuda.Event()
 
     def e2e_step():
         main = torch.cuda.current_stream(dev)
@@ -451,58 +458,61 @@ def our_arm(args):
         with torch.cuda.stream(s_in):
             a = a_h.to(dev, non_blocking=True)
             x = x_h.to(dev, non_blocking=True)
+            ev_ax.record(s_in)
             a_s, x_s = as_h.to(dev, non_blocking=True), xs_h.to(dev, non_blocking=True)
-            ev_in[chunks].record(s_in)  # a, x and the stress arguments
+            g_s = gs_h.to(dev, non_blocking=True)
+            ev_stress_in.record(s_in)
             for i in range(chunks):
                 r = slice(*bounds[i])
                 g_dev[r].copy_(g_h[r], non_blocking=True)
-                ev_in[i].record(s_in)
-            g_s = gs_h.to(dev, non_blocking=True)
-            ev_in[chunks + 1].record(s_in)
+                ev_g[i].record(s_in)
         with torch.cuda.stream(s_comp):
-            s_comp.wait_event(ev_in[chunks])
-            for t in (a, x, a_s, x_s, g_s):
+            s_comp.wait_event(ev_ax)
+            for t in (a, x):
                 t.record_stream(s_comp)
             xr = x.detach().requires_grad_(True)
-            asr, xsr = a_s.detach().requires_grad_(True), x_s.detach().requires_grad_(True)
             ars, ys_ = [], []
-            for i in range(chunks + 1):
-                if i < chunks:
-                    ar = a[slice(*bounds[i])].detach().requires_grad_(True)
-                    y = sf.regularized_gamma_p(ar, xr)
-                    ars.append(ar)
-                else:
-                    y = sf.regularized_gamma_p(asr, xsr)
+            for i in range(chunks):
+                ar = a[slice(*bounds[i])].detach().requires_grad_(True)
+                y = sf.regularized_gamma_p(ar, xr)
+                ars.append(ar)
                 ys_.append(y)
                 ev_y[i].record(s_comp)
                 with torch.cuda.stream(s_out):
                     s_out.wait_event(ev_y[i])
                     y.record_stream(s_out)
-                    dst = y_host[slice(*bounds[i])] if i < chunks else ys_host
-                    dst.copy_(y.detach(), non_blocking=True)
+                    y_host[slice(*bounds[i])].copy_(y.detach(), non_blocking=True)
+            s_comp.wait_event(ev_stress_in)
+            for t in (a_s, x_s, g_s):
+                t.record_stream(s_comp)
+            asr, xsr = a_s.detach().requires_grad_(True), x_s.detach().requires_grad_(True)
+            ys = sf.regularized_gamma_p(asr, xsr)
+            gas, gxs = torch.autograd.grad(ys, (asr, xsr), g_s)
+            ev_stress_out.record(s_comp)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_stress_out)
+                for t in (ys, gas, gxs):
+                    t.record_stream(s_out)
+                ys_host.copy_(ys.detach(), non_blocking=True)
+                gas_host.copy_(gas, non_blocking=True)
+                gxs_host.copy_(gxs, non_blocking=True)
             gx = torch.zeros_like(x)
             for i in range(chunks):
                 r = slice(*bounds[i])
-                s_comp.wait_event(ev_in[i])
+                s_comp.wait_event(ev_g[i])
                 ga, gxi = torch.autograd.grad(ys_[i], (ars[i], xr), g_dev[r])
                 gx += gxi
-                ev_out[i].record(s_comp)
+                ev_ga[i].record(s_comp)
                 with torch.cuda.stream(s_out):
-                    s_out.wait_event(ev_out[i])
+                    s_out.wait_event(ev_ga[i])
                     ga.record_stream(s_out)
                     ga_host[r].copy_(ga, non_blocking=True)
             if grp is not None:
                 gx = sum_over_ranks(gx, grp)
-            s_comp.wait_event(ev_in[chunks + 1])
-            gas, gxs = torch.autograd.grad(ys_[chunks], (asr, xsr), g_s)
-            ev_out[chunks].record(s_comp)
         with torch.cuda.stream(s_out):
-            s_out.wait_event(ev_out[chunks])
-            for t in (gx, gas, gxs):
-                t.record_stream(s_out)
+            s_out.wait_stream(s_comp)
+            gx.record_stream(s_out)
             gx_host.copy_(gx, non_blocking=True)
-            gas_host.copy_(gas, non_blocking=True)
-            gxs_host.copy_(gxs, non_blocking=True)
         main.wait_stream(s_out)
 
     t_e2e = timed_steps(e2e_step, args.steps, 2, flush)
@@ -571,8 +581,9 @@ def our_arm(args):
         },
         "e2e": {
             "value": total / t_e2e / 1e9,
-            "pipeline": f"{chunks} row chunks over 3 streams: forwards first (outputs copied out while g is copied in), "
-            "then each chunk's backward as its slice of g arrives",
+            "pipeline": f"{chunks} row chunks over 3 streams: a, x in, the grid's forwards (outputs copied out while the "
+            "rest comes in); the stress points in, forward + backward, results out; then each chunk's backward as its "
+            "slice of g arrives",
             "check_vs_device_step": e2e_check,
             "unit": "Gelem/s",
             "h2d_bytes_per_step": h2d,
