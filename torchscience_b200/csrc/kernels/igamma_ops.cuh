@@ -162,19 +162,27 @@ struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
   static constexpr int MIN_BLOCKS = 4;
   static constexpr int TILE_ROWS = TSB_IGFG_TR;
   static constexpr bool REDUCE = false;
+  // Float data is evaluated in FP64 here as well, and stored as float.  On
+  // the configuration-2 workload the mixed alternatives measured slower: the
+  // two-pass split of the sweep (an FP32 pass for the light elements, an
+  // FP64 pass for the rest) 0.77 ms against 0.62 ms for one FP64 pass, since
+  // the FP32 pass saves little on elements whose FP64 cost is a few series
+  // terms and one exponential; and the mixed evaluators on the 2^20
+  // transition points 118 us against 105 us.  The forward without
+  // derivatives keeps its mixed split (1.2x FP64).
   template <bool UNIFORM>
   __device__ static void eval_impl(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
     const double sgn = UPPER ? -1.0 : 1.0;
     const IgPre P = IgammaFwdGrad::pre(in, A, X);
-    // in[] are T: float data takes the mixed evaluators (igamma_eval_m)
+    const double a = (double)in[0], x = (double)in[1];
     if (!(mask & 2u)) {
-      const IgammaOut o = igamma_eval<0, UPPER, UNIFORM>(r, in[0], in[1], P);
+      const IgammaOut o = igamma_eval<0, UPPER, UNIFORM>(r, a, x, P);
       out[0] = (T)(UPPER ? o.q : o.p);
       out[1] = T(0);
-      out[2] = (T)(sgn * igamma_px_only((double)in[0], (double)in[1], P));
+      out[2] = (T)(sgn * igamma_px_only(a, x, P));
       return;
     }
-    const IgammaOut o = igamma_eval<1, UPPER, UNIFORM>(r, in[0], in[1], P);
+    const IgammaOut o = igamma_eval<1, UPPER, UNIFORM>(r, a, x, P);
     out[0] = (T)(UPPER ? o.q : o.p);
     out[1] = (T)(sgn * o.pa);
     out[2] = (T)(sgn * o.px);
@@ -184,37 +192,6 @@ struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
   }
   __device__ static void eval(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
     eval_impl<false>(r, in, out, mask, A, X);
-  }
-  // Two-pass sweep of float data: pass 1 the FP32 elements (compact FP32
-  // code alone in its kernel), pass 2 the rest in FP64.
-  static constexpr bool SPLIT = sizeof(T) == 4;
-  // Saturated elements (P or Q exactly 0 or 1, every derivative 0) take the
-  // first pass.
-  __device__ static bool fp64_pass(int r, const T* in, uint32_t mask, const double* A, const double* X) {
-    return !(mask & 2u) || (r != kIgSat0 && r != kIgSat1 &&
-                            igamma_needs_fp64_1(r, (float)in[1], IgammaFwdGrad::pre(in, A, X), UPPER));
-  }
-  template <int PASS>
-  __device__ static void eval_pass(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
-    const double sgn = UPPER ? -1.0 : 1.0;
-    const IgPre P = IgammaFwdGrad::pre(in, A, X);
-    IgammaOut o;
-    if constexpr (PASS == 1) {
-      o = (r == kIgSat0 || r == kIgSat1) ? igamma_saturated(r == kIgSat1)
-                                         : igamma_eval_mf1<UPPER>(r, (float)in[0], (float)in[1], P);
-    } else {
-      if (!(mask & 2u)) {
-        o = igamma_eval<0, UPPER>(r, (double)in[0], (double)in[1], P);
-        out[0] = (T)(UPPER ? o.q : o.p);
-        out[1] = T(0);
-        out[2] = (T)(sgn * igamma_px_only((double)in[0], (double)in[1], P));
-        return;
-      }
-      o = igamma_eval<1, UPPER>(r, (double)in[0], (double)in[1], P);
-    }
-    out[0] = (T)(UPPER ? o.q : o.p);
-    out[1] = (T)(sgn * o.pa);
-    out[2] = (T)(sgn * o.px);
   }
 };
 
