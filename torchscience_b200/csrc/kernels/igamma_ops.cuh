@@ -169,7 +169,7 @@ struct IgammaFwdGrad : IgammaAuxIO<1, 0, 1, T_> {
   // the FP32 pass saves little on elements whose FP64 cost is a few series
   // terms and one exponential; and the mixed evaluators on the 2^20
   // transition points 118 us against 105 us.  The forward without
-  // derivatives keeps its mixed split (1.2x FP64).
+  // derivatives keeps the mixed evaluators (1.2x FP64).
   template <bool UNIFORM>
   __device__ static void eval_impl(int r, const T* in, T* out, uint32_t mask, const double* A, const double* X) {
     const double sgn = UPPER ? -1.0 : 1.0;
