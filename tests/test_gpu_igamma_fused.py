@@ -113,6 +113,27 @@ def test_float32_data(seed):
         assert ok, report
 
 
+@pytest.mark.parametrize("which", ["p", "q"])
+@pytest.mark.parametrize("layout", ["grid", "points"])
+def test_float32_fused_forward_is_the_fp64_value_rounded_once(which, layout):
+    """The fused forward evaluates float32 data with the FP64 evaluators and
+    stores float32: its values equal the FP64 kernel's at the same inputs,
+    rounded once, bit for bit, on the row-sorted sweep (grid) and on the map
+    kernel (independent points at the transition x ~ a)."""
+    if layout == "grid":
+        a, x = inputs((192, 1), (1, 160), dtype=torch.float32, seed=21)
+    else:
+        a, _ = inputs((8192,), (1,), dtype=torch.float32, seed=22)
+        x = (a.double() * (1.0 + (torch.rand(8192, device="cuda", dtype=torch.float64,
+                                             generator=torch.Generator(device="cuda").manual_seed(23)) * 2 - 1)
+                           * 1e-2)).float()
+    ar, xr = a.clone().requires_grad_(True), x.clone().requires_grad_(True)
+    y32 = OPS[which](ar, xr)
+    y64 = OPS[which](a.double().requires_grad_(True), x.double().requires_grad_(True))
+    assert y32.dtype == torch.float32
+    assert torch.equal(y32.detach(), y64.detach().float())
+
+
 def test_double_backward_through_the_fused_path():
     gen = torch.Generator(device="cuda").manual_seed(4)
     a = (torch.rand(5, 1, device="cuda", dtype=torch.float64, generator=gen) * 5 + 0.3).requires_grad_()
